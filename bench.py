@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: DOF-updates/s per RK stage of the nonlinear Hall workload on B200.
+
+Workload (one "step" = one full solve: 260 CarpenterKennedy2N54 time steps of 5 RK stages
+each, from the initial state to t = 0.5): circularly polarised whistler wave B = (0.1 sin(z - t), 0.1 cos(z - t), 1) of the Hall induction
+equation, zero ion velocity, rho = 1, periodic [0, 2 pi]^3 on 64^3 nodes, FP64, 6th-order
+classical SBP operator plus high-order artificial dissipation (factor 1), dt = 0.5/260
+(260 steps to t = 0.5).  Inputs are synthetic (the analytic wave); the reference publishes
+no benchmark dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs an independent replica (weak scaling; a single 64^3 solve
+does not shard without a halo exchange).  value = all ranks' DOF-updates / max-over-ranks
+device time.  `--impl reference` times the reference's own kernels compiled for the host
+cores (oracle/_ref; the numpy port if that build is absent) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 64
+T_FINAL = 0.5
+NUM_STEPS_FULL = 260            # ceil(T / (0.2 dx^2)) with dx = 2 pi / 64
+DT = T_FINAL / NUM_STEPS_FULL
+STAGES = 5
+WORKLOAD = ("hall_circular_wave 64^3 periodic [0,2pi]^3, FP64, 6th-order classical SBP + high-order "
+            "dissipation (factor 1), Hall term, u=0, rho=1, CarpenterKennedy2N54, dt=0.5/260")
+METRIC = "DOF-updates/s per RK stage"
+L2_NOTE = ("L2 flushed between timed solves (256 MiB memset on the solver stream, outside the events); "
+           "within a solve the 64^3 fields stay L2 resident, as in production")
+# algorithmic bytes per node of one fused CK2N54 Hall stage kernel with J = curl(B)/rho
+# materialised by its own kernel: read b1, J, b2 (3 x 24 B), write b2, b1' (2 x 24 B)
+STAGE_BYTES_PER_NODE = 5 * 24
+CURL_BYTES_PER_NODE = 24 + 8 + 24
+
+
+def maps(n=N_GRID):
+    from inductioneq_b200.induction_eq import Maps
+    m = Maps()
+    m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": 0.0, "XMAX": 2 * math.pi,
+                     "YMIN": 0.0, "YMAX": 2 * math.pi, "ZMIN": 0.0, "ZMAX": 2 * math.pi})
+    m.I_TI.update({"DT": DT, "time_integrator": "CarpenterKennedy2N54", "final_time": T_FINAL})
+    m.I_IEq.update({"hall_term": "USE_HALL", "dissipation": "USE_ARTIFICIAL_DISSIPATION",
+                    "dissipation_form": "USE_HIGH_ORDER_DISSIPATION", "HO_DISSIPATION_FACTOR": 1.0})
+    m.I_RunOps.update({"order": 6, "testcase": "hall_circular_wave", "periodic": "USE_PERIODIC"})
+    return m
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of the GPU with the given UUID while the timed region runs."""
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9 or (self.uuid and self.uuid not in p[0]):
+                continue
+            rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------ CPU arms
+def cpu_reference_run(steps: int, warmup: int, budget_s: float | None = None):
+    """The reference's own kernels (oracle/_ref, OpenMP over all host cores) on the same
+    workload, one RK step per timed step; returns (DOF-updates/s per stage, cores, kind, sample)."""
+    import numpy as np
+
+    from oracle import refimpl
+    from oracle.sequencing import rk_step
+    cores = os.cpu_count() or 1
+    v = refimpl.Variant(order=6, testcase="hall_circular_wave", periodic=True, hall=True, dissipation="HIGH_ORDER")
+    n = N_GRID
+    nodes = (n, n, n)
+    try:
+        mesh = refimpl.Mesh(nodes, (0.0,) * 3, (2 * math.pi,) * 3, periodic=True)
+        mesh.dt = DT
+        r = refimpl.RefRunner(v, mesh, nthreads=cores)
+        kind = "reference"
+    except Exception:
+        r = None
+        kind = "port"
+    seq = rk_step("CarpenterKennedy2N54", True, False)
+    if r is None:
+        from oracle.numpy_oracle import NumpyOracle, OracleConfig
+        cfg = OracleConfig(nodes=nodes, xmin=(0.0,) * 3, xmax=(2 * math.pi,) * 3, order=6, periodic=True, hall=True,
+                           dissipation="HIGH_ORDER", testcase="hall_circular_wave", dt=DT)
+        r = NumpyOracle(cfg)
+        cores = 1
+    b, b2, cb, u = r.vec(), r.vec(), r.vec(), r.vec()
+    rho = r.scalar(fill=1.0)
+    t = np.zeros(2)
+    r.run("init_b", nodes, b)
+    for _ in range(warmup):
+        r.run_list(seq, nodes, b, b2, cb, u, rho, t)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        r.run_list(seq, nodes, b, b2, cb, u, rho, t)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s and done >= 3:
+            break
+    el = time.perf_counter() - t0
+    value = 3 * n ** 3 * STAGES * done / el
+    sample = f"{done} CK2N54 RK steps ({done * STAGES} stages) of the 64^3 workload"
+    return value, cores, kind, sample, el / done * NUM_STEPS_FULL
+
+
+# ------------------------------------------------------------------------------ main
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        # each timed step is a bounded sample (5 RK steps) of one solve; ms_per_step is
+        # scaled to the full 260-step solve
+        value, cores, kind, sample, s_per_step = cpu_reference_run(5 * a.steps, a.warmup)
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic whistler wave)",
+            "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "stages_per_step": STAGES},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    m = maps()
+    ctx = m.context(device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    nn = ctx.n
+    b, b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho = ctx.scalar()
+    tbuf = ctx.scalar(np.zeros(2), n=2)
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", u)
+    ctx.kernel("init_rho", rho)
+    b0 = ctx.get_vec(b)
+    flush = ctx.alloc(256 << 20)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def solve():
+        b.upload(b0)
+        tbuf.upload(np.zeros(2))
+
+    # ---------------- warm-up (graph capture happens on the first call)
+    for _ in range(a.warmup):
+        solve()
+        ctx.time_steps(b, b2, None, cb, u, rho, tbuf, NUM_STEPS_FULL)
+    ctx.synchronize()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.5)
+
+    # ---------------- timed region: K full solves (graph-launched steps), L2 flushed between
+    K = a.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(K):
+        solve()
+        ctx.memset(flush, k & 0xFF)
+        ev[k][0].record(stream)
+        ctx.time_steps(b, b2, None, cb, u, rho, tbuf, NUM_STEPS_FULL)
+        ev[k][1].record(stream)
+    ctx.synchronize()
+    res = ctx.results(b, T_FINAL, ctx.vec(), ctx.scalar())   # stated L2 error of the timed solve
+    # dominant-kernel timing inside the same region: per-kernel events of profiled steps
+    prof = []
+    solve()
+    for k in range(20):
+        ctx.memset(flush, k & 0xFF)
+        prof.append(ctx.profile_step(b, b2, None, cb, u, rho, tbuf))
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    step_ms = [s_.elapsed_time(e_) for s_, e_ in ev]
+    t_total = sum(step_ms) * 1e-3
+    t_max = t_total
+    if world > 1:
+        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    dof = 3 * nn * STAGES * NUM_STEPS_FULL * K * world
+    value = dof / t_max
+    stage_ms = [ms for rec in prof for (nm, ms) in rec if nm.startswith("stage")]
+    curl_ms = [ms for rec in prof for (nm, ms) in rec if nm == "curl_rho"]
+    stage_avg = statistics.mean(stage_ms) * 1e-3
+    curl_avg = statistics.mean(curl_ms) * 1e-3
+
+    # ---------------- end to end through the C ABI with host buffers (pinned): per solve,
+    # the initial state goes host -> device and the final state device -> host
+    h_b = torch.empty((ctx.n_pad, 4), dtype=torch.float64, pin_memory=True)
+    h_b.copy_(torch.from_numpy(b0))
+    h_t = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+    h_out = torch.empty_like(h_b)
+    Ke = K
+    eev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(Ke)]
+    h2d = h_b.numel() * 8 + 16
+    d2h = h_b.numel() * 8
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(Ke):
+        ctx.memset(flush, k & 0xFF)
+        eev[k][0].record(stream)
+        ctx._check(ctx.lib.ieq_upload(ctx.h, b.ptr, h_b.data_ptr(), h_b.numel() * 8))
+        ctx._check(ctx.lib.ieq_upload(ctx.h, tbuf.ptr, h_t.data_ptr(), 16))
+        ctx.time_steps(b, b2, None, cb, u, rho, tbuf, NUM_STEPS_FULL)
+        ctx._check(ctx.lib.ieq_download(ctx.h, h_out.data_ptr(), b.ptr, h_out.numel() * 8))
+        eev[k][1].record(stream)
+    ctx.synchronize()
+    e2e_t = sum(s_.elapsed_time(e_) for s_, e_ in eev) * 1e-3
+    if world > 1:
+        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_value = 3 * nn * STAGES * NUM_STEPS_FULL * Ke * world / e2e_t
+
+    # ---------------- roofline of the dominant kernel (fused stage kernel)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = STAGE_BYTES_PER_NODE * nn / stage_avg / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_stage<double, 6th classical, periodic, Hall, HOD> (fused CK2N54 a+b)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_src, "traffic": None,
+                "algorithmic_bytes_per_node": STAGE_BYTES_PER_NODE, "nodes_per_launch": nn,
+                "avg_launch_ms": stage_avg * 1e3, "curl_kernel_avg_ms": curl_avg * 1e3,
+                "note": "per-kernel CUDA events of profiled steps in the timed region, L2 flushed before each step"}
+    traffic_file = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.isfile(traffic_file):
+        with open(traffic_file) as f:
+            roofline["traffic"] = json.load(f).get("bytes_per_launch")
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
+        "ms_per_step": t_max / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (analytic whistler wave)",
+        "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "rk_steps_per_step": NUM_STEPS_FULL,
+                   "stages_per_rk_step": STAGES, "step": "one full solve to t=0.5 (260 RK steps)",
+                   "l2": L2_NOTE, "replicas": world},
+        "e2e": {"value": e2e_value, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "ieq_upload (pinned host) + ieq_time_steps(260) + ieq_download per solve"},
+        "gpu_launches": (2 * STAGES * NUM_STEPS_FULL + 1) * K + (2 * STAGES + 1) * len(prof),
+        "roofline": roofline,
+        "l2_error": {"rel": res["rel_err"], "abs": res["abs_err"], "t": T_FINAL, "steps": NUM_STEPS_FULL,
+                     "divergence_norm": res["divergence_norm"]},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cv, cores, kind, sample, _ = cpu_reference_run(10 ** 6, 1, budget_s=15.0)
+        out["cpu_baseline"] = {"value": cv, "unit": "DOF/s", "cores": cores, "kind": kind, "sample": sample}
+    if rank == 0:
+        print(json.dumps(out))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,156 @@
+/* inductioneq.h -- C ABI of the B200 (sm_100a) InductionEq time-stepping library.
+ *
+ * Drop-in boundary for the reference's MatCL-driven OpenCL kernels
+ * (IANW-Projects/InductionEq v1.1.1).  The reference host (MATLAB) compiles a list of
+ * source files with a "-DKEY=VAL" settings string and then runs lists of named kernels
+ * that all receive the same argument vector:
+ *     cl_run_kernel(device, kernel_path_list, settings)            -- compile
+ *     t = cl_run_kernel(device, names, g_range, l_range, args..., 0) -- run
+ * (matlab/+induction_eq/compute_numerical_solution.m:23,179-181; the MatCL mex itself is
+ * not part of the reference).  This header replaces that pair:
+ *     ieq_create(settings, kernel_path_list)   <- cl_run_kernel(dev, paths, settings)
+ *     ieq_run_kernels(names, g_range, args)    <- cl_run_kernel(dev, names, g, l, args..., 0)
+ * plus one typed entry point per reference kernel (inductioneq_kernels.h) and the fused,
+ * graph-captured paths that the B200 build adds (time stepping, CG cleaning, norms).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Field arguments are DEVICE pointers in the
+ *     reference layout: a vector field is REAL4 AoS (x,y,z,w; w = 0) of num_nodes_pad
+ *     entries, a scalar field num_nodes_pad REALs, `time` two REALs
+ *     (time[0] = start of the step, time[1] = stage time).  Node index
+ *     idx = ix + NX*(iy + NY*iz) (include/utils.h:66-68).
+ *   - REAL is double unless the settings say -DREAL=float.
+ *   - Every function returns ieq_status; ieq_last_error() describes the last failure.
+ *   - One CUDA stream per context; calls on one context are not thread safe, separate
+ *     contexts are independent.  Work is asynchronous on that stream unless stated.
+ */
+#ifndef INDUCTIONEQ_H
+#define INDUCTIONEQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ieq_status {
+  IEQ_OK = 0,
+  IEQ_ERR_SETTINGS = 1,       /* unknown/contradictory -D settings or kernel path list   */
+  IEQ_ERR_SHAPE = 2,          /* grid too small for the operator, bad g_range           */
+  IEQ_ERR_CUDA = 3,           /* a CUDA runtime call failed                              */
+  IEQ_ERR_NAN = 4,            /* a non-finite value was detected in a result             */
+  IEQ_ERR_NOT_CONVERGED = 5,  /* CG stopped at max_iterations above the threshold        */
+  IEQ_ERR_TIMEOUT = 6,        /* a bounded device wait gave up                           */
+  IEQ_ERR_UNKNOWN_KERNEL = 7, /* a kernel name the reference does not define             */
+  IEQ_ERR_ARG = 8             /* null/misaligned pointer, wrong argument count           */
+} ieq_status;
+
+typedef struct ieq_ctx ieq_ctx;
+
+/* Create a context from the reference's settings string and kernel path list.
+ * settings: the concatenation generate_settings.m produces (" -DNODES_X=40 -DDX=5.1e-02
+ *   -DUSE_UIBJ_PRODUCT=1 ... -cl-mad-enable"); OpenCL compiler options are accepted and
+ *   ignored.  Keys this library adds (all optional): -DIEQ_INTEGRATOR=<name of one of the
+ *   six integrators> (host-side I_TI('time_integrator')), -DIEQ_VARIABLE_U=1
+ *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>,
+ *   -DIEQ_MIXED_CG=1 (FP64 CG vectors and reductions while REAL=float).
+ * kernel_paths: the kernel_path_list (compute_numerical_solution_setup.m:57-122).  Only
+ *   the base names matter: the operator header ({2,4,6}thOrder[Extended].h) selects the SBP
+ *   operator, "<testcase>.h" the testcase, artificial_dissipation.cl enables dissipation.
+ * device: CUDA device ordinal. */
+ieq_status ieq_create(ieq_ctx **ctx, const char *settings, const char *const *kernel_paths,
+                      int n_paths, int device);
+void ieq_destroy(ieq_ctx *ctx);
+const char *ieq_last_error(const ieq_ctx *ctx);
+const char *ieq_status_string(ieq_status s);
+
+/* Sizes the reference host derives in initialize.m:31-48. */
+size_t ieq_num_nodes(const ieq_ctx *ctx);
+size_t ieq_num_nodes_pad(const ieq_ctx *ctx);
+size_t ieq_num_groups(const ieq_ctx *ctx);
+int ieq_real_size(const ieq_ctx *ctx); /* 8 (double) or 4 (float) */
+
+/* Device memory owned by the context (freed by ieq_free or ieq_destroy).  Memory
+ * allocated elsewhere (e.g. by PyTorch) may be passed to every call as well. */
+ieq_status ieq_alloc(ieq_ctx *ctx, size_t bytes, void **dptr);
+ieq_status ieq_free(ieq_ctx *ctx, void *dptr);
+ieq_status ieq_upload(ieq_ctx *ctx, void *dst, const void *host_src, size_t bytes);
+ieq_status ieq_download(ieq_ctx *ctx, void *host_dst, const void *src, size_t bytes);
+ieq_status ieq_memset(ieq_ctx *ctx, void *dst, int value, size_t bytes);
+ieq_status ieq_synchronize(ieq_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work. */
+void *ieq_stream(ieq_ctx *ctx);
+
+/* MatCL-form list call: enqueue every kernel of `names` in order, each with the same
+ * argument vector `args` (device pointers, n_args of them).  g_range as in the reference
+ * host (3D node range, or {num_nodes_pad,1,1} for the reductions, or the CG interior
+ * range NODES-2*BNODES).  If elapsed_seconds is not NULL the call synchronises and
+ * returns the device time of the list (cudaEvent), like MatCL's return value. */
+ieq_status ieq_run_kernels(ieq_ctx *ctx, const char *const *names, int n_names,
+                           const uint32_t g_range[3], void *const *args, int n_args,
+                           double *elapsed_seconds);
+
+/* The same with HOST arrays, copied in before and back after the list, in place, as the
+ * MatCL mex does with MATLAB arrays.  arg_bytes[i] is the size of host array i. */
+ieq_status ieq_run_kernels_host(ieq_ctx *ctx, const char *const *names, int n_names,
+                                const uint32_t g_range[3], void *const *host_args,
+                                const size_t *arg_bytes, int n_args, double *elapsed_seconds);
+
+/* ---------------------------------------------------------------- fused B200 paths */
+
+/* num_steps time steps of the configured integrator (-DIEQ_INTEGRATOR), the loop of
+ * compute_numerical_solution.m:174-192, with the stage kernels fused as far as the data
+ * flow allows and the step captured in a CUDA graph.  Field arguments as for the
+ * reference kernels of that integrator (b3 is ignored by the 2N schemes and may be NULL).
+ * Results equal running rk_step() kernel lists through ieq_run_kernels. */
+ieq_status ieq_time_steps(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
+                          void *rho, void *time, int num_steps);
+
+/* Divergence cleaning, matlab/+induction_eq/clean_div.m:36-79, device resident: CG on
+ * (-Laplace) phi = div B over the interior, stopping when the unweighted squared
+ * residual <= absolute_error_threshold^2 or after max_iterations, then B is projected.
+ * The CG vectors and reductions are FP64 when REAL=double or -DIEQ_MIXED_CG=1.
+ * Returns IEQ_ERR_NOT_CONVERGED (with B still projected) if the cap was hit. */
+ieq_status ieq_clean_div(ieq_ctx *ctx, void *b, int max_iterations,
+                         double absolute_error_threshold, int *iterations,
+                         double *residual_norm2, double *initial_divergence_norm);
+
+/* Mass-weighted squared norms (kernel_operator.cl:11-137), reduced on the device in a
+ * fixed order (bitwise reproducible) and returned to the host in FP64. */
+ieq_status ieq_norm2_value(ieq_ctx *ctx, const void *vec_field, double *result);
+ieq_status ieq_norm2_diff_value(ieq_ctx *ctx, const void *vec_a, const void *vec_b,
+                                double *result);
+ieq_status ieq_norm2_S_value(ieq_ctx *ctx, const void *scalar_field, double *result);
+ieq_status ieq_dot_value(ieq_ctx *ctx, const void *a, const void *b, double *result);
+
+/* Result metrics of compute_numerical_solution.m:198-250 at time t: abs/rel L2 error
+ * against b_analytical(t), ||div B|| and the energy.  work_vec/work_scalar are scratch
+ * fields of the context's layout. */
+typedef struct ieq_results {
+  double abs_err, rel_err, divergence_norm, energy;
+} ieq_results;
+ieq_status ieq_compute_results(ieq_ctx *ctx, const void *b, double t, void *work_vec,
+                               void *work_scalar, ieq_results *out);
+
+/* IEQ_ERR_NAN if any x/y/z component of the vector field is not finite, else IEQ_OK. */
+ieq_status ieq_check_finite(ieq_ctx *ctx, const void *vec_field);
+
+/* Profiling: one time step of ieq_time_steps launched without a graph, with a CUDA event
+ * after every kernel; records[k] gets the kernel's label and device duration (ms), in
+ * launch order (the kernel time MatCL returns, per kernel).  Synchronises. */
+typedef struct ieq_kernel_record {
+  char name[40];
+  double ms;
+} ieq_kernel_record;
+ieq_status ieq_profile_step(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
+                            void *rho, void *time, int max_records, ieq_kernel_record *records,
+                            int *n_records);
+
+#ifdef __cplusplus
+}
+#endif
+
+#include "inductioneq_kernels.h"
+
+#endif /* INDUCTIONEQ_H */

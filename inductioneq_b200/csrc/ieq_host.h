@@ -1,0 +1,97 @@
+// ieq_host.h -- host-side context of the InductionEq library (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/inductioneq.h"
+
+namespace ieq {
+
+// The reference's -D settings (generate_settings.m) in runtime form.
+struct Settings {
+  int nodes[3] = {0, 0, 0};
+  double d[3] = {0, 0, 0};
+  double xmin[3] = {0, 0, 0}, xmax[3] = {0, 0, 0};
+  bool have_d[3] = {false, false, false};
+  double dt = 0.0;
+  bool real_float = false;
+  int w_size = 1;
+  // operator header
+  int order = 0;
+  bool extended = false;
+  // flux forms: 0 CENTRAL, 1 SPLIT, 2 PRODUCT, 3 ZERO; -1 unset
+  int uibj = -1, source = -1, ujbi = -1;
+  bool hall = false, periodic = false;
+  bool dissipation = false;
+  int diss_form = 0;   // 0 none, 1 high order, 2 first order, 3 adaptive
+  double hod_factor = 1.0, mp2min = 0, mp2max = 0, cmin = 0, cmax = 0;
+  int laplace = 0;     // 0 WS_D0, 1 NS_D0, 2 WS_LN
+  int bnodes = -1;
+  bool reduce = false;
+  int testcase = -1;
+  double omega = 1.0;
+  std::string integrator;
+  bool variable_u = false;
+};
+
+// parse helpers (settings.cpp)
+bool parse_settings(const char *settings, const char *const *paths, int n_paths, Settings &out,
+                    std::string &err);
+int integrator_id(const std::string &name);
+
+struct SbpRows {
+  int nb = 0, width = 0;
+  std::vector<double> rows;   // (2nb+1) x width
+  double at(int r, int c) const { return rows[(size_t)r * width + c]; }
+};
+struct SbpOperator {
+  int order = 0, nb = 0, sw = 0, w_hod = 0;
+  SbpRows D, Dadj, DHO, lap[3];
+  std::vector<double> minv;
+  bool has_lap[3] = {false, false, false};
+};
+bool load_operator(int order, bool extended, SbpOperator &op, std::string &err);
+
+}  // namespace ieq
+
+struct ieq_ctx {
+  ieq::Settings s;
+  ieq::SbpOperator op;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  size_t n = 0, n_pad = 0, n_groups = 0;
+  int op_id = 0;
+  // device tables
+  void *d_tables = nullptr;        // Tables<REAL>
+  void *d_rows_r = nullptr;        // D, Dadj rows in REAL  [2][rows*sw]
+  double *d_rows_d = nullptr;      // D, Dadj rows in FP64
+  void *d_lap_r = nullptr;         // Laplacian rows in REAL
+  double *d_lap_d = nullptr;       // Laplacian rows in FP64
+  void *d_wnorm = nullptr;         // per-axis norm weights in REAL (nx + ny + nz)
+  // scratch
+  double *d_partials = nullptr;    // reduction partials
+  double *d_partials2 = nullptr;
+  double *d_total = nullptr;       // reduction totals
+  unsigned *d_counter = nullptr;   // last-block tickets
+  int *d_flag = nullptr;
+  void *d_cg = nullptr;            // CgState
+  double *d_cg_vec = nullptr;      // FP64 CG vectors: div, phi, r, u, lap (5 x n_pad)
+  double *d_cg_hist = nullptr;
+  int cg_hist_len = 0;
+  void *d_pingpong = nullptr;      // second b1 buffer of the fused 2N step
+  std::set<void *> allocs;
+  // fused time-step graphs keyed by the argument pointers
+  struct GraphEntry {
+    cudaGraphExec_t exec1 = nullptr, exec2 = nullptr;
+  };
+  std::map<std::vector<uintptr_t>, GraphEntry> graphs;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-kernel event records of ieq_profile_step (label, event after the launch)
+  std::vector<std::pair<std::string, cudaEvent_t>> *recorder = nullptr;
+};

@@ -1,0 +1,476 @@
+// misc_kernels.cuh -- the non-stage kernels: testcase evaluation, time bookkeeping,
+// pointwise Runge-Kutta updates, reductions (norms, dot products), divergence/gradient
+// operators and the conjugate-gradient pieces of divergence cleaning.
+#pragma once
+#include "ieq_common.cuh"
+
+namespace ieq {
+
+// ---------------------------------------------------------------- testcase evaluation
+enum InitKind : int { INIT_B = 0, INIT_U = 1, INIT_RHO = 2, ANALYTICAL_B = 3, CALC_U = 4 };
+
+// kernel_init.cl:3-48 and kernel_time_integrator.cl:93-125 (u = u_analytical(time[1]))
+template <typename R>
+__global__ void k_init(Mesh m, int tc, int kind, R4<R> *vout, R *sout, const R *time) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= m.nx || iy >= m.ny || iz >= m.nz) return;
+  const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+  switch (kind) {
+    case INIT_B: st3(vout + idx, b_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
+    case INIT_U: st3(vout + idx, u_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
+    case INIT_RHO: sout[idx] = (R)1; break;
+    case ANALYTICAL_B: st3(vout + idx, b_analytical<R>(tc, m, ix, iy, iz, time[0])); break;
+    case CALC_U: st3(vout + idx, u_analytical<R>(tc, m, ix, iy, iz, time[1])); break;
+  }
+}
+
+// ---------------------------------------------------------------- time bookkeeping
+// the idx == 0 branches of the "a" kernels and calc_time_*: one thread
+template <typename R>
+__global__ void k_time(R *time, int kind, R K, R DT) {
+  if (kind == 1) {
+    time[1] = time[0] + K;
+  } else if (kind == 2) {
+    const R t0 = time[0] + DT;
+    time[0] = t0;
+    time[1] = t0;
+  }
+}
+
+// ---------------------------------------------------------------- pointwise RK updates
+enum PointwiseMode : int {
+  PW_AXPY = 0,        // P = P + c1*Q                     (2N "b" kernels: b1 += B*b2)
+  PW_2R = 1,          // P = P + c1*D; Q = P + c2*D       (2R "b" kernels)
+  PW_SSP104_06 = 2,   // b3 = 0.04 b1 + 0.36 b2; b2 = 0.6 b1 + 0.4 b2
+};
+
+template <typename R>
+__global__ void k_pointwise(long long n, int mode, R4<R> *P, R4<R> *Q, R4<R> *Dd, R c1, R c2, R *time,
+                            int tkind, R tK, unsigned *counter) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) {
+    if (mode == PW_AXPY) {
+      const V3<R> p = ld3_plain(P + i), q = ld3_plain(Q + i);
+      st3(P + i, V3<R>{p.x + c1 * q.x, p.y + c1 * q.y, p.z + c1 * q.z});
+    } else if (mode == PW_2R) {
+      const V3<R> p = ld3_plain(P + i), d = ld3_plain(Dd + i);
+      const V3<R> pn = {p.x + c1 * d.x, p.y + c1 * d.y, p.z + c1 * d.z};
+      st3(P + i, pn);
+      st3(Q + i, V3<R>{pn.x + c2 * d.x, pn.y + c2 * d.y, pn.z + c2 * d.z});
+    } else {
+      // P = b1, Q = b2, Dd = b3
+      const V3<R> b1 = ld3_plain(P + i), b2 = ld3_plain(Q + i);
+      st3(Dd + i, V3<R>{(R)0.04 * b1.x + (R)0.36 * b2.x, (R)0.04 * b1.y + (R)0.36 * b2.y,
+                        (R)0.04 * b1.z + (R)0.36 * b2.z});
+      st3(Q + i, V3<R>{(R)0.60 * b1.x + (R)0.40 * b2.x, (R)0.60 * b1.y + (R)0.40 * b2.y,
+                       (R)0.60 * b1.z + (R)0.40 * b2.z});
+    }
+  }
+  if (tkind != 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(counter, 1u) == gridDim.x - 1) {
+        if (tkind == 1) {
+          time[1] = time[0] + tK;
+        }
+        __threadfence();
+        *counter = 0u;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- reductions
+// Deterministic two-pass sums: a fixed grid of blocks writes one FP64 partial each (fixed
+// element-to-thread assignment, warp-shuffle tree), then one block adds the partials in a
+// fixed order.  Reruns are bitwise identical.
+enum ReduceKind : int { RED_NORM2 = 0, RED_NORM2_DIFF = 1, RED_NORM2_S = 2, RED_DOT = 3 };
+
+template <typename T>
+struct ReduceArgs {
+  int kind;
+  long long n;          // nodes (padding entries are zero and skipped)
+  int nx, ny;
+  const R4<T> *va, *vb;
+  const T *sa, *sb;
+  const T *wx, *wy, *wz;  // per-axis mass weights (REAL)D/M_INV[row] (kernel_operator.cl:26-28)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ double reduce_term(const ReduceArgs<T> &a, long long i) {
+  if (a.kind == RED_DOT) return (double)(a.sa[i] * a.sb[i]);
+  const int ix = (int)(i % a.nx);
+  const long long r = i / a.nx;
+  const int iy = (int)(r % a.ny);
+  const int iz = (int)(r / a.ny);
+  const T fac = (a.wx[ix] * a.wy[iy]) * a.wz[iz];
+  if (a.kind == RED_NORM2_S) return (double)((fac * a.sa[i]) * a.sa[i]);
+  V3<T> v = ld3(a.va + i);
+  if (a.kind == RED_NORM2_DIFF) {
+    const V3<T> w = ld3(a.vb + i);
+    v = {v.x - w.x, v.y - w.y, v.z - w.z};
+  }
+  return (double)(fac * ((v.x * v.x + v.y * v.y) + v.z * v.z));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_partials(const ReduceArgs<T> a, double *partials) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n; i += stride)
+    acc += reduce_term(a, i);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+  }
+}
+
+// sum of `np` partials in a fixed order by one block; the total goes to *total (FP64) and,
+// if out_real is given, to out_real[0] with zeros in out_real[1..n_zero-1]
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_final(const double *partials, int np, double *total, T *out_real,
+                                                      long long n_zero, int accumulate) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sm[w];
+    if (total) *total = v;
+    if (out_real) out_real[0] = accumulate ? (T)((double)out_real[0] + v) : (T)v;
+  }
+  if (out_real && !accumulate)
+    for (long long i = 1 + threadIdx.x; i < n_zero; i += blockDim.x) out_real[i] = (T)0;
+}
+
+// ---------------------------------------------------------------- operators
+// Generic-row SBP operators for the diagnostics and divergence cleaning.  R is the
+// precision of the vector field, S the precision of scalar fields and arithmetic.
+struct OpDesc {
+  int nb, sw;          // derivative rows
+  int periodic;
+};
+
+template <typename R, typename S>
+struct OpArgs {
+  Mesh m;
+  OpDesc op;
+  int off;                  // BNODES offset of the CG interior range
+  int gx, gy, gz;           // NDRange
+  const R4<R> *v;           // vector input
+  const S *s;               // scalar input
+  R4<R> *vout;
+  S *sout;
+  const S *D;               // derivative rows [2nb+1][sw] in S
+  const S *Dadj;
+  S dS[3];                  // (S)DX ...
+  int adjoint;              // projector with the least-norm Laplacian
+};
+
+template <typename S>
+__device__ __forceinline__ int nbr_rt(int i, int o, int n, int periodic) {
+  int j = i + o;
+  if (periodic) {
+    j += (j < 0) ? n : 0;
+    j -= (j >= n) ? n : 0;
+  } else if (j < 0 || j >= n) {
+    j = i;
+  }
+  return j;
+}
+
+// d/d(axis) of one component (comp < 0: scalar field) with rows `tab`, divided by (S)d
+template <typename R, typename S>
+__device__ S diff_rt(const OpArgs<R, S> &a, const S *tab, int ax, int comp, int ix, int iy, int iz) {
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
+  const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
+  const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  const int row = a.op.periodic ? a.op.nb : sbp_row(ii[ax], nn[ax], a.op.nb);
+  const int c0 = (a.op.sw - 1) / 2;
+  S v = 0;
+  for (int c = 0; c < a.op.sw; ++c) {
+    const S cf = tab[row * a.op.sw + c];
+    if (cf == (S)0) continue;
+    const long long j = idx + (long long)(nbr_rt<S>(ii[ax], c - c0, nn[ax], a.op.periodic) - ii[ax]) * st[ax];
+    S f;
+    if (comp < 0) f = a.s[j];
+    else {
+      const R *p = reinterpret_cast<const R *>(a.v + j);
+      f = (S)p[comp];
+    }
+    v += cf * f;
+  }
+  return v / a.dS[ax];
+}
+
+// div (kernel_operator.cl:145, kernel_div_cleaning.cl:60 with off = BNODES)
+template <typename R, typename S>
+__global__ void k_div(const OpArgs<R, S> a) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
+  if (ix >= a.gx + a.off || iy >= a.gy + a.off || iz >= a.gz + a.off) return;
+  const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  a.sout[idx] = (diff_rt(a, a.D, 0, 0, ix, iy, iz) + diff_rt(a, a.D, 1, 1, ix, iy, iz)) +
+                diff_rt(a, a.D, 2, 2, ix, iy, iz);
+}
+
+// grad (kernel_operator.cl:170) and the projector (kernel_div_cleaning.cl:96-109):
+// mode 0 writes grad(s) to vout; mode 1 adds it to vout.xyz; mode 2 subtracts grad_adj
+template <typename R, typename S>
+__global__ void k_grad(const OpArgs<R, S> a, int mode) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= a.gx || iy >= a.gy || iz >= a.gz) return;
+  const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  const S *tab = mode == 2 ? a.Dadj : a.D;
+  const S gx = diff_rt(a, tab, 0, -1, ix, iy, iz);
+  const S gy = diff_rt(a, tab, 1, -1, ix, iy, iz);
+  const S gz = diff_rt(a, tab, 2, -1, ix, iy, iz);
+  if (mode == 0) {
+    st3(a.vout + idx, V3<R>{(R)gx, (R)gy, (R)gz});
+  } else {
+    V3<R> b = ld3_plain(a.vout + idx);
+    if (mode == 1) b = {(R)((S)b.x + gx), (R)((S)b.y + gy), (R)((S)b.z + gz)};
+    else b = {(R)((S)b.x - gx), (R)((S)b.y - gy), (R)((S)b.z - gz)};
+    R *p = reinterpret_cast<R *>(a.vout + idx);
+    p[0] = b.x; p[1] = b.y; p[2] = b.z;   // .w untouched, as the reference's .xyz store
+  }
+}
+
+// ---------------------------------------------------------------- conjugate gradients
+template <typename S>
+struct LapArgs {
+  Mesh m;
+  int nb, w, periodic, off, gx, gy, gz;
+  const S *L;          // rows [2nb+1][w]
+  S dd[3];             // (S)DX*(S)DX ...
+  const S *in;
+  S *out;
+  double *partials;    // CG: block partials of <in, out>
+};
+
+// (-Laplace) of kernel_div_cleaning.cl:11-56 at one node, in the reference's order
+template <typename S>
+__device__ __forceinline__ S laplace_at(const LapArgs<S> &a, int ix, int iy, int iz, long long idx) {
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
+  const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
+  int row[3];
+  for (int ax = 0; ax < 3; ++ax) row[ax] = a.periodic ? a.nb : sbp_row(ii[ax], nn[ax], a.nb);
+  const int c0 = (a.w - 1) / 2;
+  S val = 0;
+  for (int c = 0; c < a.w; ++c) {
+    S t[3];
+    for (int ax = 0; ax < 3; ++ax) {
+      const S cf = a.L[row[ax] * a.w + c];
+      const long long j = idx + (long long)(nbr_rt<S>(ii[ax], c - c0, nn[ax], a.periodic) - ii[ax]) * st[ax];
+      t[ax] = (cf * a.in[j]) / a.dd[ax];
+    }
+    val = ((val + t[0]) + t[1]) + t[2];
+  }
+  return val;
+}
+
+// calc_laplace_divcleaning over the CG interior (kernel_div_cleaning.cl:75-84)
+template <typename S>
+__global__ void __launch_bounds__(256) k_laplace(const LapArgs<S> a) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
+  if (ix >= a.gx + a.off || iy >= a.gy + a.off || iz >= a.gz + a.off) return;
+  const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  a.out[idx] = laplace_at(a, ix, iy, iz, idx);
+}
+
+// x = a*x + y (calc_axpy, kernel_CG.cl:8) or x = x + a*y (calc_xpay, kernel_CG.cl:21) over
+// the interior; `a` is a device scalar as in the reference
+template <typename S>
+__global__ void k_axpy_interior(Mesh m, int off, int gx, int gy, int gz, S *x, const S *y, const S *a, int xpay,
+                                S sign) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
+  if (ix >= gx + off || iy >= gy + off || iz >= gz + off) return;
+  const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+  const S av = sign * a[0];
+  x[idx] = xpay ? x[idx] + av * y[idx] : av * x[idx] + y[idx];
+}
+
+// ---- device-resident CG loop (matlab/+induction_eq/clean_div.m:47-73).  The scalars live
+// in CgState; every kernel returns at once when `done` is set, so a fixed-length chunk of
+// iterations can be replayed from a CUDA graph and stops exactly where the host loop would.
+// The dot products are fused into the stencil/update kernels: each block writes a partial,
+// and the last block to finish (ticket counter) adds the partials in a fixed order.
+struct CgState {
+  double rr;         // residual_norm2
+  double old;        // old_residual_norm2
+  double tol;        // absolute_error_threshold^2
+  double alpha;
+  int it;            // iterations
+  int max_it;
+  int done;
+  int pad;
+};
+
+// u = beta*u + r with beta = rr/old (calc_axpy over the I_DC g_range)
+template <typename S>
+__global__ void k_cg_direction(Mesh m, int off, int gx, int gy, int gz, S *u, const S *r, const CgState *cs) {
+  if (cs->done) return;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
+  if (ix >= gx + off || iy >= gy + off || iz >= gz + off) return;
+  const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+  const S beta = (S)(cs->rr / cs->old);
+  u[idx] = beta * u[idx] + r[idx];
+}
+
+// sum of np partials in a fixed order by the calling block (all threads get the total)
+__device__ __forceinline__ double block_sum_partials(const double *partials, int np) {
+  __shared__ double sm[32];
+  __shared__ double total;
+  const int tx = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  double acc = 0.0;
+  for (int i = tx; i < np; i += nt) acc += partials[i];
+  acc = warp_sum(acc);
+  if ((tx & 31) == 0) sm[tx >> 5] = acc;
+  __syncthreads();
+  if (tx == 0) {
+    double v = 0.0;
+    for (int w = 0; w < nt >> 5; ++w) v += sm[w];
+    total = v;
+  }
+  __syncthreads();
+  return total;
+}
+
+// block partial of v, written to partials[block]; returns true in the last block to finish
+__device__ __forceinline__ bool block_partial_and_ticket(double v, double *partials, unsigned *counter) {
+  __shared__ double sm[32];
+  __shared__ bool last;
+  const int tx = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  v = warp_sum(v);
+  if ((tx & 31) == 0) sm[tx >> 5] = v;
+  __syncthreads();
+  if (tx == 0) {
+    double s = 0.0;
+    for (int w = 0; w < nt >> 5; ++w) s += sm[w];
+    partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+    __threadfence();
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    last = atomicAdd(counter, 1u) == nb - 1;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// lap = (-Laplace) u over the interior; alpha = rr / <u, lap> (last block)
+template <typename S>
+__global__ void __launch_bounds__(256) k_cg_laplace(const LapArgs<S> a, CgState *cs, unsigned *counter) {
+  if (cs->done) return;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
+  double prod = 0.0;
+  if (ix < a.gx + a.off && iy < a.gy + a.off && iz < a.gz + a.off) {
+    const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+    const S val = laplace_at(a, ix, iy, iz, idx);
+    a.out[idx] = val;
+    prod = (double)a.in[idx] * (double)val;
+  }
+  if (block_partial_and_ticket(prod, a.partials, counter)) {
+    const int np = gridDim.x * gridDim.y * gridDim.z;
+    const double ul = block_sum_partials(a.partials, np);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+      cs->alpha = cs->rr / ul;
+      *counter = 0u;
+    }
+  }
+}
+
+// phi += alpha*u; r -= alpha*lap; rr = <r, r> (last block), then the loop condition
+template <typename S>
+__global__ void __launch_bounds__(256) k_cg_update(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,
+                                                   const S *u, const S *lap, double *partials, CgState *cs,
+                                                   unsigned *counter, double *history) {
+  if (cs->done) return;
+  const S alpha = (S)cs->alpha;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
+  double rr = 0.0;
+  if (ix < gx + off && iy < gy + off && iz < gz + off) {
+    const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+    phi[idx] = phi[idx] + alpha * u[idx];
+    const S rn = r[idx] + (-alpha) * lap[idx];
+    r[idx] = rn;
+    rr = (double)rn * (double)rn;
+  }
+  if (block_partial_and_ticket(rr, partials, counter)) {
+    const int np = gridDim.x * gridDim.y * gridDim.z;
+    const double tot = block_sum_partials(partials, np);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+      cs->old = cs->rr;
+      cs->rr = tot;
+      cs->it += 1;
+      if (history) history[cs->it] = tot;
+      cs->done = !(tot > cs->tol && cs->it < cs->max_it);
+      *counter = 0u;
+    }
+  }
+}
+
+// initial residual r = div B: rr = <r, r> from reduction partials, and the loop condition
+__global__ void k_cg_start(const double *partials_rr, int np, CgState *cs, double *history) {
+  const double rr = block_sum_partials(partials_rr, np);
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    cs->rr = rr;
+    cs->old = 1.0;
+    cs->it = 0;
+    if (history) history[0] = rr;
+    cs->done = !(rr > cs->tol && cs->it < cs->max_it);
+  }
+}
+
+// any non-zero x/y/z component (decides whether the convection terms can vanish)
+template <typename R>
+__global__ void k_any_nonzero(long long n, const R4<R> *v, int *flag) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3<R> x = ld3(v + i);
+  if (x.x != (R)0 || x.y != (R)0 || x.z != (R)0) *flag = 1;
+}
+
+// finiteness check of a vector field (sets *flag if any x/y/z is not finite)
+template <typename R>
+__global__ void k_check_finite(long long n, const R4<R> *v, int *flag) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3<R> x = ld3(v + i);
+  if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z)) *flag = 1;
+}
+
+}  // namespace ieq

@@ -1,0 +1,42 @@
+// stage_inst.cuh -- instantiates the stage and curl kernels for one (REAL, operator) pair.
+// Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so the instantiations
+// compile in parallel.
+#include "stage_kernel.cuh"
+
+namespace ieq {
+
+template <>
+void launch_stage<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R> &a, bool per, bool hall, int diss, dim3 grid,
+                                 dim3 block, cudaStream_t s) {
+#define IEQ_L(P, H, D) k_stage<IEQ_R, IEQ_OP, P, H, D><<<grid, block, 0, s>>>(a)
+  if (per) {
+    if (hall) {
+      if (diss == DISS_NONE) IEQ_L(true, true, DISS_NONE);
+      else if (diss == DISS_HO) IEQ_L(true, true, DISS_HO);
+      else IEQ_L(true, true, DISS_FO_OR_AD);
+    } else {
+      if (diss == DISS_NONE) IEQ_L(true, false, DISS_NONE);
+      else if (diss == DISS_HO) IEQ_L(true, false, DISS_HO);
+      else IEQ_L(true, false, DISS_FO_OR_AD);
+    }
+  } else {
+    if (hall) {
+      if (diss == DISS_NONE) IEQ_L(false, true, DISS_NONE);
+      else if (diss == DISS_HO) IEQ_L(false, true, DISS_HO);
+      else IEQ_L(false, true, DISS_FO_OR_AD);
+    } else {
+      if (diss == DISS_NONE) IEQ_L(false, false, DISS_NONE);
+      else if (diss == DISS_HO) IEQ_L(false, false, DISS_HO);
+      else IEQ_L(false, false, DISS_FO_OR_AD);
+    }
+  }
+#undef IEQ_L
+}
+
+template <>
+void launch_curl<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R> &a, bool per, dim3 grid, dim3 block, cudaStream_t s) {
+  if (per) k_curl_rho<IEQ_R, IEQ_OP, true><<<grid, block, 0, s>>>(a);
+  else k_curl_rho<IEQ_R, IEQ_OP, false><<<grid, block, 0, s>>>(a);
+}
+
+}  // namespace ieq

@@ -1,0 +1,438 @@
+// stage_kernel.cuh -- the fused Runge-Kutta stage kernel and the curl(B)/rho kernel.
+//
+// One thread per node.  For every node the kernel evaluates the time derivative DB of
+// kernel/kernel_time_integrator.cl:9-31 -- volume terms (induction_Eq_volume.cl),
+// Hall volume term, SAT surface terms (induction_Eq_surface.cl) and artificial
+// dissipation (artificial_dissipation.cl) -- and applies the stage update of the
+// integrator in the same pass (epilogue modes below), so the stage derivative never
+// touches memory.
+//
+// Volume term.  The reference sums the split-form flux F(B_m,u_m,B_k,u_k) over the
+// stencil points k of each derivative row.  Every flux form is bilinear in (m, k)
+// quantities, so with D applied to the pointwise products the sum factors into
+//     sum_k c_k F = w1 D[u_i B_a] + w2 B_a,m D[u_i] + w3 u_i,m D[B_a]
+//                 - (v1 D[u_a B_i] + v2 u_a,m D[B_i] + v3 B_i,m D[u_a])
+// (plus terms proportional to sum_k c_k, which is zero for every derivative row);
+// w and v come from the USE_UIBJ_* / USE_SOURCE_* / USE_UJBI_* switches.  This cuts the
+// flops per stencil point from ~40 to 9-21 and changes only the rounding order.
+//
+// Interior nodes of every axis use the interior row (radius RI = ORDER/2, coefficients
+// in kernel parameters); the SBP boundary closures read their rows from a table.
+#pragma once
+#include "ieq_common.cuh"
+
+namespace ieq {
+
+enum EpilogueMode : int {
+  EP_X_PLUS_HF = 0,   // out = X + h*F                 SSPRK33_1, SSPRK104, KCL_5, CFR_6
+  EP_PX_QYHF = 1,     // out = p*X + q*(Y + h*F)       SSPRK33_2b/3b, SSPRK104_11b
+  EP_HF = 2,          // out = h*F                     *_1a, KCL/CFR "a" kernels
+  EP_AX_HF = 3,       // out = A*X + h*F               CarpenterKennedy/ToulorgeDesmet "a"
+  EP_2N_FUSED = 4,    // t = A*X + h*F; out = t; out2 = Z + Bc*t     ("a" and "b" fused)
+  EP_2N_FUSED_FIRST = 5,  // t = h*F; out = t; out2 = Z + Bc*t
+};
+
+enum TimePost : int {
+  TP_NONE = 0,
+  TP_SET_STAGE = 1,   // time[1] = time[0] + K
+  TP_ADVANCE = 2,     // time[0] = time[0] + DT; time[1] = time[0]
+};
+
+enum DissKind : int { DISS_NONE = 0, DISS_HO = 1, DISS_FO_OR_AD = 2 };
+
+template <typename R>
+struct StageArgs {
+  Mesh m;
+  const R4<R> *bk;      // field the derivative is taken of
+  const R4<R> *J;       // curl(B)/rho (Hall)
+  const R4<R> *u;
+  const R4<R> *X, *Y, *Z;
+  R4<R> *out, *out2;
+  const Tables<R> *tab;
+  R *time;
+  unsigned *counter;    // last-block ticket for the time post-update
+  R Dint[7];            // interior derivative row, offsets -RI..RI
+  R Hint[7];            // interior dissipation row, offsets -RI..RI
+  R two_inv_d[3];       // (REAL)(2.0/DX) ...
+  R inv_d[3];           // (REAL)(1.0/DX) ...
+  R sat_s[3];           // (REAL)(M_INV[0]/DX) ...
+  R dR[3];              // (REAL)DX ...
+  R w[6];               // flux-form weights w1 w2 w3 v1 v2 v3
+  int need;             // 1: D[u_i B_a], 2: D[u], 4: D[B], 8: D[u_a B_i]
+  int conv;             // convection terms present (u not identically zero) ...
+  const int *conv_flag; // ... or, if set, read from device memory at kernel start
+  int tc;               // testcase (b_boundary of the inflow SAT)
+  int diss_form;        // 2 first order, 3 adaptive (DISS_FO_OR_AD)
+  R hod_factor;
+  double mp2min, mp2max, cmin, cmax;
+  int mode;
+  R p, q, h, A, Bc;
+  int tpost;
+  R tK, tDT;
+};
+
+// neighbour index along one axis: periodic wrap, or clamp-to-self outside the grid
+// (include/utils.h:89-168; the coefficient of a clamped point is zero)
+template <bool PER>
+__device__ __forceinline__ int nbr(int i, int o, int n) {
+  int j = i + o;
+  if (PER) {
+    j += (j < 0) ? n : 0;
+    j -= (j >= n) ? n : 0;
+  } else {
+    j = (j < 0 || j >= n) ? i : j;
+  }
+  return j;
+}
+
+template <typename R>
+struct AxisSums {
+  V3<R> SuiBa, SU, SB, SuaB, SH, SHo;
+};
+
+template <typename R, bool HALL, bool HOD>
+__device__ __forceinline__ void accumulate(AxisSums<R> &s, const StageArgs<R> &a, int conv, int axis, R cD, R cH,
+                                           long long j) {
+  const V3<R> B = ld3(a.bk + j);
+  if (conv && cD != (R)0) {
+    const V3<R> U = ld3(a.u + j);
+    const R Ba = axis == 0 ? B.x : (axis == 1 ? B.y : B.z);
+    const R Ua = axis == 0 ? U.x : (axis == 1 ? U.y : U.z);
+    if (a.need & 1) {
+      s.SuiBa.x += cD * (U.x * Ba); s.SuiBa.y += cD * (U.y * Ba); s.SuiBa.z += cD * (U.z * Ba);
+    }
+    if (a.need & 2) { s.SU.x += cD * U.x; s.SU.y += cD * U.y; s.SU.z += cD * U.z; }
+    if (a.need & 4) { s.SB.x += cD * B.x; s.SB.y += cD * B.y; s.SB.z += cD * B.z; }
+    if (a.need & 8) {
+      s.SuaB.x += cD * (Ua * B.x); s.SuaB.y += cD * (Ua * B.y); s.SuaB.z += cD * (Ua * B.z);
+    }
+  }
+  if (HALL && cD != (R)0) {
+    // Hall_volume: D[J_a B - J B_a]
+    const V3<R> Jk = ld3(a.J + j);
+    const R Ja = axis == 0 ? Jk.x : (axis == 1 ? Jk.y : Jk.z);
+    const R Ba = axis == 0 ? B.x : (axis == 1 ? B.y : B.z);
+    s.SH.x += cD * (Ja * B.x - Jk.x * Ba);
+    s.SH.y += cD * (Ja * B.y - Jk.y * Ba);
+    s.SH.z += cD * (Ja * B.z - Jk.z * Ba);
+  }
+  if (HOD && cH != (R)0) {
+    s.SHo.x += cH * B.x; s.SHo.y += cH * B.y; s.SHo.z += cH * B.z;
+  }
+}
+
+// first-order / adaptive dissipation (artificial_dissipation.cl:36-160), evaluated as in
+// the reference per stencil point; used only by the DISS_FO_OR_AD instantiation.
+template <typename R, int OP, bool PER>
+__device__ V3<R> fo_ad_dissipation(const StageArgs<R> &a, const int ii[3], const int nn[3],
+                                   const long long st[3], long long idx, V3<R> Bm, V3<R> um) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH;
+  V3<R> acc = {0, 0, 0};
+  const bool adaptive = a.diss_form == 3;
+  auto kap = [&](unsigned k, R dx, R b1, R b2, R u1, R u2) -> R {
+    // include/artificial_dissipation.h:23-45 (k*k of the unsigned argument)
+    R s = (fmax(fabs(u1), fabs(u2)) * (b1 - b2)) * (b1 - b2);
+    k = k + (k == 0);
+    double kk = (double)(k * k);
+    double lo = ((kk * a.mp2min) * a.cmin) * (double)dx;
+    double hi = ((kk * a.mp2max) * a.cmax) * (double)dx;
+    double sd = (double)s;
+    double v = ((lo < sd) && (sd < hi)) * sqrt(fabs(sd - lo) / fabs(hi - lo)) + (double)(sd >= hi);
+    return (R)v;
+  };
+  for (int ax = 0; ax < 3; ++ax) {
+    const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
+    V3<R> tmp = {0, 0, 0};
+    for (int c = 0; c < SW; ++c) {
+      const int o = c - C0;
+      const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+      const R cd = fabs(a.tab->D[row][c]);
+      const V3<R> Bk = ld3(a.bk + j);
+      const V3<R> uk = ld3(a.u + j);
+      V3<R> sg = {fmax(fabs(uk.x), fabs(um.x)), fmax(fabs(uk.y), fabs(um.y)), fmax(fabs(uk.z), fabs(um.z))};
+      if (adaptive) {
+        const unsigned k = (unsigned)(o < 0 ? -o : o);
+        tmp.x += ((cd * kap(k, a.dR[ax], Bk.x, Bm.x, uk.x, um.x)) * sg.x) * (Bk.x - Bm.x);
+        tmp.y += ((cd * kap(k, a.dR[ax], Bk.y, Bm.y, uk.y, um.y)) * sg.y) * (Bk.y - Bm.y);
+        tmp.z += ((cd * kap(k, a.dR[ax], Bk.z, Bm.z, uk.z, um.z)) * sg.z) * (Bk.z - Bm.z);
+      } else {
+        tmp.x += (cd * sg.x) * (Bk.x - Bm.x);
+        tmp.y += (cd * sg.y) * (Bk.y - Bm.y);
+        tmp.z += (cd * sg.z) * (Bk.z - Bm.z);
+      }
+    }
+    acc.x += tmp.x / a.dR[ax]; acc.y += tmp.y / a.dR[ax]; acc.z += tmp.z / a.dR[ax];
+  }
+  if (adaptive) {
+    // high-order part weighted by (1 - kappa) of the neighbouring pair
+    for (int term = -WH + 1; term <= 0; ++term) {
+      for (int ax = 0; ax < 3; ++ax) {
+        const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
+        const long long j1 = idx + (long long)(nbr<PER>(ii[ax], term + WH - 1, nn[ax]) - ii[ax]) * st[ax];
+        const long long j2 = idx + (long long)(nbr<PER>(ii[ax], term + WH - 2, nn[ax]) - ii[ax]) * st[ax];
+        const V3<R> b1 = ld3(a.bk + j1), b2 = ld3(a.bk + j2), u1 = ld3(a.u + j1), u2 = ld3(a.u + j2);
+        // diff_HOD (artificial_dissipation.h:58-101) for this start offset
+        const R sgn = (Op<OP>::ORDER / 2 + 1) % 2 ? (R)-1 : (R)1;
+        V3<R> hod = {0, 0, 0};
+        for (int i = 0; i < WH; ++i) {
+          const R coef = ((a.tab->Minv[row] * a.tab->DHO[row][term + WH - 1]) * a.tab->DHO[NB][i]) * sgn;
+          const long long j = idx + (long long)(nbr<PER>(ii[ax], i + term, nn[ax]) - ii[ax]) * st[ax];
+          const V3<R> Bk = ld3(a.bk + j);
+          hod.x += coef * Bk.x; hod.y += coef * Bk.y; hod.z += coef * Bk.z;
+        }
+        acc.x += (((R)1 - kap(1, a.dR[ax], b1.x, b2.x, u1.x, u2.x)) * a.hod_factor) * hod.x;
+        acc.y += (((R)1 - kap(1, a.dR[ax], b1.y, b2.y, u1.y, u2.y)) * a.hod_factor) * hod.y;
+        acc.z += (((R)1 - kap(1, a.dR[ax], b1.z, b2.z, u1.z, u2.z)) * a.hod_factor) * hod.z;
+      }
+    }
+  }
+  return acc;
+}
+
+template <typename R, int OP, bool PER, bool HALL, int DISS>
+__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH;
+  constexpr int RI = Op<OP>::RI;
+  constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
+  constexpr bool HOD = DISS == DISS_HO;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const bool active = ix < nx && iy < ny && iz < nz;
+  if (active) {
+    const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
+    const int ii[3] = {ix, iy, iz};
+    const int nn[3] = {nx, ny, nz};
+    const long long st[3] = {1, nx, (long long)nx * ny};
+    const int conv = a.conv_flag ? *a.conv_flag : a.conv;
+    const V3<R> Bm = ld3(a.bk + idx);
+    V3<R> um = {0, 0, 0};
+    if (conv) um = ld3(a.u + idx);
+    V3<R> db = {0, 0, 0};
+    V3<R> hod = {0, 0, 0};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      AxisSums<R> s{};
+      const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
+      if (row == NB) {
+#pragma unroll
+        for (int o = -RI; o <= RI; ++o) {
+          const R cD = a.Dint[o + RI];
+          const R cH = a.Hint[o + RI];
+          long long j = idx;
+          if (o != 0) {
+            if (PER) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+            else j = idx + (long long)o * st[ax];
+          }
+          accumulate<R, HALL, HOD>(s, a, conv, ax, cD, cH, j);
+        }
+      } else {
+        for (int o = -RB; o <= RB; ++o) {
+          const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+          const R cH = (HOD && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+          if (cD == (R)0 && cH == (R)0) continue;
+          const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+          accumulate<R, HALL, HOD>(s, a, conv, ax, cD, cH, j);
+        }
+      }
+      if (conv) {
+        const R Ba = ax == 0 ? Bm.x : (ax == 1 ? Bm.y : Bm.z);
+        const R Ua = ax == 0 ? um.x : (ax == 1 ? um.y : um.z);
+        const R SBa = ax == 0 ? s.SB.x : (ax == 1 ? s.SB.y : s.SB.z);
+        const R SUa = ax == 0 ? s.SU.x : (ax == 1 ? s.SU.y : s.SU.z);
+        const R *w = a.w;
+        V3<R> vol;
+        vol.x = w[0] * s.SuiBa.x + w[1] * Ba * s.SU.x + w[2] * um.x * SBa -
+                (w[3] * s.SuaB.x + w[4] * Ua * s.SB.x + w[5] * Bm.x * SUa);
+        vol.y = w[0] * s.SuiBa.y + w[1] * Ba * s.SU.y + w[2] * um.y * SBa -
+                (w[3] * s.SuaB.y + w[4] * Ua * s.SB.y + w[5] * Bm.y * SUa);
+        vol.z = w[0] * s.SuiBa.z + w[1] * Ba * s.SU.z + w[2] * um.z * SBa -
+                (w[3] * s.SuaB.z + w[4] * Ua * s.SB.z + w[5] * Bm.z * SUa);
+        db.x += a.two_inv_d[ax] * vol.x;
+        db.y += a.two_inv_d[ax] * vol.y;
+        db.z += a.two_inv_d[ax] * vol.z;
+      }
+      if (HALL) {
+        db.x += a.inv_d[ax] * s.SH.x;
+        db.y += a.inv_d[ax] * s.SH.y;
+        db.z += a.inv_d[ax] * s.SH.z;
+      }
+      if (HOD) {
+        hod.x += s.SHo.x; hod.y += s.SHo.y; hod.z += s.SHo.z;
+      }
+    }
+    // ---- SAT surface terms on the faces of a non-periodic box
+    if (!PER) {
+      const bool face = ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1;
+      if (face) {
+        if (HALL) {
+          // induction_Eq_surface.cl:35-81 (outflow, directional do-nothing)
+          const V3<R> Jm = ld3(a.J + idx);
+          const V3<R> tv = {(R)0.5 * um.x - Jm.x, (R)0.5 * um.y - Jm.y, (R)0.5 * um.z - Jm.z};
+          for (int ax = 0; ax < 3; ++ax) {
+            const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
+            if (!l && !r) continue;
+            const R tva = ax == 0 ? tv.x : (ax == 1 ? tv.y : tv.z);
+            const R Ba = ax == 0 ? Bm.x : (ax == 1 ? Bm.y : Bm.z);
+            const R c1 = (l && tva > (R)0 ? (R)-1 : (R)0) + (r && tva < (R)0 ? (R)1 : (R)0);
+            const R c2 = (l ? (R)-1 : (R)0) + (r ? (R)1 : (R)0);
+            const R f1 = c1 * tva, f2 = c2 * Ba;
+            db.x += a.sat_s[ax] * (f1 * Bm.x + f2 * Jm.x);
+            db.y += a.sat_s[ax] * (f1 * Bm.y + f2 * Jm.y);
+            db.z += a.sat_s[ax] * (f1 * Bm.z + f2 * Jm.z);
+          }
+        } else if (conv) {
+          // induction_Eq_surface.cl:7-33 (upwind inflow against b_boundary(t))
+          const R t = a.time[1];
+          const V3<R> bb = b_boundary<R>(a.tc, a.m, ix, iy, iz, t);
+          const V3<R> df = {Bm.x - bb.x, Bm.y - bb.y, Bm.z - bb.z};
+          for (int ax = 0; ax < 3; ++ax) {
+            const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
+            const R ua = ax == 0 ? um.x : (ax == 1 ? um.y : um.z);
+            const R c = (l && ua > (R)0 ? (R)-1 : (R)0) + (r && ua < (R)0 ? (R)1 : (R)0);
+            if (c == (R)0) continue;
+            const R f = (a.sat_s[ax] * c) * ua;
+            db.x += f * df.x; db.y += f * df.y; db.z += f * df.z;
+          }
+        }
+      }
+    }
+    if (HOD) {
+      db.x += a.hod_factor * hod.x;
+      db.y += a.hod_factor * hod.y;
+      db.z += a.hod_factor * hod.z;
+    }
+    if (DISS == DISS_FO_OR_AD) {
+      const V3<R> ds = fo_ad_dissipation<R, OP, PER>(a, ii, nn, st, idx, Bm, um);
+      db.x += ds.x; db.y += ds.y; db.z += ds.z;
+    }
+    // ---- stage update
+    V3<R> r;
+    switch (a.mode) {
+      case EP_X_PLUS_HF: {
+        const V3<R> X = ld3_plain(a.X + idx);
+        r = {X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
+        st3(a.out + idx, r);
+        break;
+      }
+      case EP_PX_QYHF: {
+        const V3<R> X = ld3_plain(a.X + idx), Y = ld3_plain(a.Y + idx);
+        r = {a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
+             a.p * X.z + a.q * (Y.z + a.h * db.z)};
+        st3(a.out + idx, r);
+        break;
+      }
+      case EP_HF:
+        st3(a.out + idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
+        break;
+      case EP_AX_HF: {
+        const V3<R> X = ld3_plain(a.X + idx);
+        st3(a.out + idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
+        break;
+      }
+      case EP_2N_FUSED:
+      case EP_2N_FUSED_FIRST: {
+        V3<R> t;
+        if (a.mode == EP_2N_FUSED) {
+          const V3<R> X = ld3_plain(a.X + idx);
+          t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
+        } else {
+          t = {a.h * db.x, a.h * db.y, a.h * db.z};
+        }
+        st3(a.out + idx, t);
+        const V3<R> Z = ld3_plain(a.Z + idx);
+        st3(a.out2 + idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
+        break;
+      }
+    }
+  }
+  // ---- time bookkeeping of the folded "a"/calc_time kernels, done by the last block
+  if (a.tpost != TP_NONE) {
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+      __threadfence();
+      const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+      const unsigned ticket = atomicAdd(a.counter, 1u);
+      if (ticket == nblocks - 1) {
+        if (a.tpost == TP_SET_STAGE) {
+          a.time[1] = a.time[0] + a.tK;
+        } else {
+          const R t0 = a.time[0] + a.tDT;
+          a.time[0] = t0;
+          a.time[1] = t0;
+        }
+        __threadfence();
+        *a.counter = 0u;
+      }
+    }
+  }
+}
+
+// curl(b)/rho (kernel_time_integrator.cl:136-208 via SBP_operator.cl:126-135), with the
+// same interior/boundary row split; diff_* divide by (REAL)DX as the reference does.
+template <typename R>
+struct CurlArgs {
+  Mesh m;
+  const R4<R> *b;
+  const R *rho;       // nullptr: plain curl (kernel_operator.cl:158 calc_curl)
+  R4<R> *out;
+  const Tables<R> *tab;
+  R dR[3];
+  R Dint[7];
+};
+
+template <typename R, int OP, bool PER>
+__global__ void __launch_bounds__(256) k_curl_rho(const __grid_constant__ CurlArgs<R> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= a.m.nx || iy >= a.m.ny || iz >= a.m.nz) return;
+  const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
+  const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
+  V3<R> g[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    V3<R> v = {0, 0, 0};
+    const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
+    if (row == NB) {
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) {
+        const R c = a.Dint[o + RI];
+        if (o == 0) continue;   // the interior row has a zero centre
+        long long j;
+        if (PER) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+        else j = idx + (long long)o * st[ax];
+        const V3<R> B = ld3(a.b + j);
+        v.x += c * B.x; v.y += c * B.y; v.z += c * B.z;
+      }
+    } else {
+      for (int o = -C0; o <= C0; ++o) {
+        const R c = a.tab->D[row][o + C0];
+        if (c == (R)0) continue;
+        const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+        const V3<R> B = ld3(a.b + j);
+        v.x += c * B.x; v.y += c * B.y; v.z += c * B.z;
+      }
+    }
+    g[ax] = {v.x / a.dR[ax], v.y / a.dR[ax], v.z / a.dR[ax]};
+  }
+  V3<R> c = {g[1].z - g[2].y, g[2].x - g[0].z, g[0].y - g[1].x};
+  if (a.rho) {
+    const R r = a.rho[idx];
+    c = {c.x / r, c.y / r, c.z / r};
+  }
+  st3(a.out + idx, c);
+}
+
+// explicit launchers, instantiated per (R, OP) in stage_<r>_o<op>.cu
+template <typename R, int OP>
+void launch_stage(const StageArgs<R> &a, bool per, bool hall, int diss, dim3 grid, dim3 block,
+                  cudaStream_t s);
+template <typename R, int OP>
+void launch_curl(const CurlArgs<R> &a, bool per, dim3 grid, dim3 block, cudaStream_t s);
+
+}  // namespace ieq

@@ -1,0 +1,158 @@
+"""Host-side mirror of the reference's MATLAB driver (matlab/+induction_eq/*.m).
+
+The reference keeps its run description in global maps (prepare_vars.m:29-56) --
+I_Mesh, I_TI, I_IEq, I_DC, I_Tech, I_RunOps -- turns the upper-case keys into an OpenCL
+"-D" settings string (generate_settings.m) and assembles the kernel path list
+(compute_numerical_solution_setup.m:57-122).  ``Maps`` carries the same keys with the same
+meanings; ``settings()`` and ``kernel_path_list()`` produce the strings that
+``inductioneq_b200.lib.Context`` (the C ABI's ieq_create) accepts, and ``initialize`` /
+``compute_numerical_solution`` / ``clean_div`` follow initialize.m,
+compute_numerical_solution.m and clean_div.m on the B200 library.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .lib import Context
+
+
+def generate_settings(m: dict, keys) -> str:
+    """generate_settings.m:3-33: USE_* values become -DUSE_*=1, integers -DKEY=%d, reals
+    -DKEY=%.16e, the 'optimizations' string is appended verbatim."""
+    out = ""
+    for k in keys:
+        if k not in m:
+            continue
+        v = m[k]
+        if isinstance(v, str):
+            if k == "optimizations":
+                out += v
+            elif "USE" in v:
+                out += f" -D{v}=1"
+            else:
+                out += f" -D{k}={v}"
+        elif isinstance(v, bool):
+            out += f" -D{k}={int(v)}"
+        elif isinstance(v, (int, np.integer)):
+            out += f" -D{k}={int(v)}"
+        else:
+            out += f" -D{k}={float(v):.16e}"
+    return out
+
+
+@dataclass
+class Maps:
+    """I_Mesh, I_TI, I_IEq, I_DC, I_Tech, I_RunOps with the reference's defaults."""
+    I_Mesh: dict = field(default_factory=lambda: {"NODES_X": 0, "NODES_Y": 0, "NODES_Z": 0, "XMIN": 0.0,
+                                                  "XMAX": 0.0, "YMIN": 0.0, "YMAX": 0.0, "ZMIN": 0.0,
+                                                  "ZMAX": 0.0})
+    I_TI: dict = field(default_factory=lambda: {"cfl": 0.0, "final_time": 0.0, "time_integrator": ""})
+    I_IEq: dict = field(default_factory=lambda: {"form_uibj": "USE_UIBJ_PRODUCT",
+                                                 "form_source": "USE_SOURCE_CENTRAL",
+                                                 "form_ujbi": "USE_UJBI_CENTRAL", "hall_term": "NONE",
+                                                 "dissipation": "NONE",
+                                                 "dissipation_form": "USE_HIGH_ORDER_DISSIPATION",
+                                                 "HO_DISSIPATION_FACTOR": 1.0, "MP2MIN": 1.0, "MP2MAX": 10.0,
+                                                 "CMIN": 1.0, "CMAX": 10.0})
+    I_DC: dict = field(default_factory=lambda: {"divergence_cleaning": False,
+                                                "divergence_cleaning_form": "USE_LAPLACE_WIDE_STENCIL_DIRICHLET",
+                                                "absolute_error_threshold": 1e-3, "max_iterations": 50})
+    I_Tech: dict = field(default_factory=lambda: {"device": 0, "REAL": "double", "W_SIZE": 1,
+                                                  "optimizations": " -cl-mad-enable -cl-no-signed-zeros"})
+    I_RunOps: dict = field(default_factory=lambda: {"order": 4, "operator_form": "classical",
+                                                    "testcase": "rotation_3D", "variable_u": False,
+                                                    "periodic": "NONE"})
+    tc_omega: float = 1.0
+
+    # initialize.m:12-21
+    def spacing(self) -> tuple[float, float, float]:
+        m = self.I_Mesh
+        per = self.I_RunOps["periodic"] == "USE_PERIODIC"
+        out = []
+        for a in "XYZ":
+            span = float(m[a + "MAX"] - m[a + "MIN"])
+            n = float(m["NODES_" + a])
+            out.append(span / n if per else span / (n - 1))
+        return tuple(out)
+
+    def settings(self) -> str:
+        """compute_numerical_solution_setup.m:97-137."""
+        m = dict(self.I_Mesh)
+        m["DX"], m["DY"], m["DZ"] = self.spacing()
+        tech = dict(self.I_Tech)
+        tech["REAL4"] = tech["REAL"] + "4"
+        s = generate_settings(self.I_IEq, ["form_uibj", "form_source", "form_ujbi", "hall_term"])
+        s += generate_settings(self.I_TI, ["DT"])
+        s += generate_settings(tech, ["REAL", "REAL4", "W_SIZE", "optimizations"])
+        s += generate_settings(m, ["DX", "DY", "DZ", "NODES_X", "NODES_Y", "NODES_Z", "XMIN", "XMAX", "YMIN",
+                                   "YMAX", "ZMIN", "ZMAX"])
+        if self.I_IEq["dissipation"] == "USE_ARTIFICIAL_DISSIPATION":
+            s += generate_settings(self.I_IEq, ["dissipation", "dissipation_form", "HO_DISSIPATION_FACTOR"])
+            if self.I_IEq["dissipation_form"] == "USE_ADAPTIVE_DISSIPATION":
+                s += generate_settings(self.I_IEq, ["MP2MIN", "MP2MAX", "CMIN", "CMAX"])
+        dc = self.I_DC
+        bn = 0 if dc["divergence_cleaning_form"] == "USE_LAPLACE_WIDE_STENCIL_LNS" else 1
+        s += generate_settings({"BNODES": bn, "divergence_cleaning_form": dc["divergence_cleaning_form"]},
+                               ["BNODES", "divergence_cleaning_form"])
+        s += generate_settings(self.I_RunOps, ["periodic"])
+        # keys of this library: integrator, variable velocity, rotation rate of the testcase
+        if self.I_TI.get("time_integrator"):
+            s += f" -DIEQ_INTEGRATOR={self.I_TI['time_integrator']}"
+        if self.I_RunOps.get("variable_u"):
+            s += " -DIEQ_VARIABLE_U=1"
+        s += f" -DTC_OMEGA={self.tc_omega:.16e}"
+        return s
+
+    def kernel_path_list(self) -> list[str]:
+        """compute_numerical_solution_setup.m:57-122."""
+        o = self.I_RunOps
+        order = o["order"]
+        hdr = f"../include/{order}{'th' if order > 2 else 'nd'}Order{'Extended' if o['operator_form'] == 'extended' else ''}.h"
+        paths = [hdr, "../include/utils.h", f"../include/{o['testcase']}.h", "../kernel/kernel_init.cl",
+                 "../kernel/SBP_operator.cl", "../kernel/kernel_operator.cl"]
+        if self.I_DC["divergence_cleaning"]:
+            paths += ["../kernel/kernel_div_cleaning.cl", "../kernel/kernel_CG.cl"]
+        if self.I_IEq["dissipation"] == "USE_ARTIFICIAL_DISSIPATION":
+            paths += ["../include/artificial_dissipation.h", "../kernel/artificial_dissipation.cl"]
+        paths += ["../kernel/induction_Eq_volume.cl", "../kernel/induction_Eq_surface.cl",
+                  "../kernel/kernel_dot_product.cl", "../kernel/kernel_time_integrator.cl"]
+        return paths
+
+    def context(self, device: int = 0) -> Context:
+        return Context(self.settings(), self.kernel_path_list(), device)
+
+
+def initialize(maps: Maps, u_max: float | None = None, device: int = 0):
+    """initialize.m: spacing, fields b/u/rho from the testcase, dt from the CFL number
+    (dt = cfl*min(d)/max|u|, num_steps = ceil(T/dt), dt = T/num_steps, lines 93-99).
+    Returns (ctx, b, u, rho) device buffers; u_max overrides max|u| (the Hall cases with
+    u = 0 need an explicit step)."""
+    maps.I_TI.setdefault("DT", 0.0)
+    ctx = maps.context(device)
+    b, u, rho = ctx.vec(), ctx.vec(), ctx.scalar()
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", u)
+    ctx.kernel("init_rho", rho)
+    if u_max is None:
+        uh = ctx.get_vec(u)
+        u_max = float(np.sqrt((uh[:, :3] ** 2).sum(1)).max())
+    dt = maps.I_TI["cfl"] * min(maps.spacing()) / u_max
+    num_steps = math.ceil(maps.I_TI["final_time"] / dt)
+    maps.I_TI["DT"] = maps.I_TI["final_time"] / num_steps
+    maps.I_TI["num_steps"] = num_steps
+    ctx.close()
+    ctx = maps.context(device)   # recompile with DT, as compute_numerical_solution does
+    return ctx
+
+
+def compute_numerical_solution(ctx: Context, b, u, rho, num_steps: int, t_final: float) -> dict:
+    """compute_numerical_solution.m: the step loop (fused, graph captured) and the results."""
+    b2, b3, cb = ctx.vec(), ctx.vec(), ctx.vec()
+    time = ctx.scalar(np.zeros(2), n=2)
+    ctx.time_steps(b, b2, b3, cb, u, rho, time, num_steps)
+    ctx.synchronize()
+    wv, ws = ctx.vec(), ctx.scalar()
+    return ctx.results(b, t_final, wv, ws)

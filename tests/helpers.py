@@ -1,0 +1,51 @@
+"""Shared helpers of the tests: contexts and oracles built from one case description."""
+from __future__ import annotations
+
+import numpy as np
+
+from inductioneq_b200.induction_eq import Maps
+from oracle.numpy_oracle import NumpyOracle, OracleConfig
+from tests.golden.cases import mesh_args, variant_kwargs
+
+INTEGRATOR_OF = {}
+
+
+def maps_for(c: dict) -> Maps:
+    m = Maps()
+    n = c["nodes"]
+    lo, hi = c["lo"], c["hi"]
+    m.I_Mesh.update({"NODES_X": n[0], "NODES_Y": n[1], "NODES_Z": n[2], "XMIN": lo, "XMAX": hi,
+                     "YMIN": lo, "YMAX": hi, "ZMIN": lo, "ZMAX": hi})
+    m.I_TI["DT"] = c.get("dt", 0.0)
+    m.I_TI["time_integrator"] = c.get("integrator", "")
+    m.I_IEq["form_uibj"] = "USE_UIBJ_" + c.get("uibj", "PRODUCT")
+    m.I_IEq["form_source"] = "USE_SOURCE_" + c.get("source", "CENTRAL")
+    m.I_IEq["form_ujbi"] = "USE_UJBI_" + c.get("ujbi", "CENTRAL")
+    m.I_IEq["hall_term"] = "USE_HALL" if c.get("hall") else "NONE"
+    d = c.get("dissipation", "NONE")
+    if d != "NONE":
+        m.I_IEq["dissipation"] = "USE_ARTIFICIAL_DISSIPATION"
+        m.I_IEq["dissipation_form"] = f"USE_{d}_DISSIPATION"
+    m.I_DC["divergence_cleaning"] = True
+    m.I_DC["divergence_cleaning_form"] = "USE_LAPLACE_" + c.get("laplace", "WIDE_STENCIL_DIRICHLET")
+    m.I_Tech["REAL"] = c.get("real", "double")
+    m.I_RunOps.update({"order": c.get("order", 4), "operator_form": "extended" if c.get("extended") else "classical",
+                       "testcase": c["testcase"], "variable_u": c.get("variable_u", False),
+                       "periodic": "USE_PERIODIC" if c.get("periodic") else "NONE"})
+    m.tc_omega = c.get("omega", 1.0)
+    return m
+
+
+def oracle_for(c: dict, dt=None) -> NumpyOracle:
+    m = mesh_args(c)
+    cfg = OracleConfig(nodes=m["nodes"], xmin=m["xmin"], xmax=m["xmax"], periodic=m["periodic"],
+                       dt=c.get("dt", 0.0) if dt is None else dt, bnodes=c.get("bnodes", 1),
+                       tc_omega=c.get("omega", 1.0),
+                       **{k: v for k, v in variant_kwargs(c).items() if k != "periodic"})
+    return NumpyOracle(cfg)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a - b| / max(|b|): the per-stage relative error of a field."""
+    scale = float(np.abs(b).max())
+    return float(np.abs(a - b).max()) / (scale if scale > 0 else 1.0)

@@ -1,0 +1,77 @@
+"""CPU tests of the C ABI: the library loads, exports every declared entry point, and
+rejects bad settings before touching a GPU (no compute calls here)."""
+from __future__ import annotations
+
+import ctypes
+
+import pytest
+
+from inductioneq_b200 import lib as L
+from inductioneq_b200.induction_eq import Maps, generate_settings
+
+
+def test_library_exports_every_declared_function():
+    so = L.load()
+    names = L.declared_functions()
+    assert len(names) > 95 + 20
+    missing = [n for n in names if not hasattr(so, n)]
+    assert not missing, missing
+
+
+def test_every_reference_kernel_has_a_typed_entry_point():
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "g", os.path.join(L.PKG, "csrc", "gen_kernel_abi.py"))
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    assert len(g.KERNELS) == 95
+    so = L.load()
+    for name, _, cite, _ in g.KERNELS:
+        assert hasattr(so, "ieq_" + name), name
+        assert cite.startswith("kernel/")
+
+
+def _create(settings, paths):
+    so = L.load()
+    h = ctypes.c_void_p()
+    arr = (ctypes.c_char_p * len(paths))(*[p.encode() for p in paths])
+    st = so.ieq_create(ctypes.byref(h), settings.encode(), arr, len(paths), 0)
+    return st, so.ieq_last_error(None).decode()
+
+
+BASE = " -DNODES_X=16 -DNODES_Y=16 -DNODES_Z=16 -DXMIN=0 -DXMAX=1 -DYMIN=0 -DYMAX=1 -DZMIN=0 -DZMAX=1"
+
+
+@pytest.mark.parametrize("settings,paths,status,msg", [
+    (BASE, ["../include/rotation_3D.h"], 1, "operator header"),
+    (BASE, ["../include/4thOrder.h"], 1, "testcase"),
+    (" -DNODES_X=16", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "lack"),
+    (BASE + " -DUSE_UIBJ_ZERO=1", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "flux form"),
+    (BASE + " -DUSE_LAPLACE_NARROW_STENCIL_DIRICHLET=1", ["../include/4thOrderExtended.h", "../include/rotation_3D.h"],
+     1, "narrow-stencil"),
+    (BASE + " -DIEQ_INTEGRATOR=RK4", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "integrator"),
+    (BASE.replace("=16", "=10"), ["../include/6thOrder.h", "../include/rotation_3D.h"], 2, "2*NUM_BOUNDS"),
+])
+def test_bad_settings_are_rejected_on_the_host(settings, paths, status, msg):
+    st, err = _create(settings, paths)
+    assert st == status, (st, err)
+    assert msg in err
+
+
+def test_generate_settings_matches_reference_format():
+    m = {"NODES_X": 40, "DX": 2.0 / 39.0, "form_uibj": "USE_UIBJ_PRODUCT", "REAL": "double",
+         "optimizations": " -cl-mad-enable"}
+    s = generate_settings(m, ["form_uibj", "NODES_X", "DX", "REAL", "optimizations"])
+    assert s == " -DUSE_UIBJ_PRODUCT=1 -DNODES_X=40 -DDX=5.1282051282051280e-02 -DREAL=double -cl-mad-enable"
+
+
+def test_maps_kernel_path_list_mirrors_setup():
+    m = Maps()
+    m.I_RunOps["order"] = 6
+    m.I_RunOps["operator_form"] = "extended"
+    m.I_IEq["dissipation"] = "USE_ARTIFICIAL_DISSIPATION"
+    p = m.kernel_path_list()
+    assert p[0] == "../include/6thOrderExtended.h"
+    assert "../kernel/artificial_dissipation.cl" in p
+    assert p[-1] == "../kernel/kernel_time_integrator.cl"

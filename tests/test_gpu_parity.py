@@ -1,0 +1,253 @@
+"""GPU parity: the sm_100a kernels against the oracle on the same seeded inputs.
+
+Tolerances: FP64 results agree with the oracle to 1e-12 relative per stage
+(max |gpu - oracle| / max |oracle| over the field, after every kernel of the step); FP32
+results to 2e-5.  The inputs are the golden fixtures (made by the reference's own kernels).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.hostloops import clean_div, norms, time_loop
+from oracle.sequencing import NUM_FIELDS, rk_step
+from tests.golden.cases import CG_CASES, STEP_CASES
+from tests.helpers import maps_for, oracle_for, rel_err
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def _golden():
+    z = np.load(GOLDEN)
+    return z, json.loads(bytes(z["manifest"]).decode())
+
+
+def tol(c):
+    return TOL32 if c.get("real") == "float" else TOL64
+
+
+class HostRunner:
+    """Runs reference kernels on the GPU through the MatCL-form host-array call."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.dtype = ctx.real
+
+    def run(self, name, grange, *arrays):
+        self.ctx.run_host([name], grange, *arrays)
+
+    def vec(self):
+        return np.zeros((self.ctx.n_pad, 4), dtype=self.dtype)
+
+    def scalar(self, fill=0.0):
+        return np.full((self.ctx.n_pad,), fill, dtype=self.dtype)
+
+    @property
+    def cfg(self):
+        class _C:
+            pass
+        c = _C()
+        c.nodes = self._nodes
+        return c
+
+
+def host_runner(ctx, nodes):
+    r = HostRunner(ctx)
+    r._nodes = tuple(nodes)
+    return r
+
+
+def _fields(ctx, o, z, name):
+    b = z[f"{name}/in_b"].astype(o.T)
+    u = z[f"{name}/in_u"].astype(o.T)
+    host = [b, np.zeros_like(b), np.zeros_like(b), np.zeros_like(b), u, np.ones(o.N, dtype=o.T),
+            np.zeros(2, dtype=o.T)]
+    dev = [ctx.vec(host[0]), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(host[4]), ctx.scalar(host[5]),
+           ctx.scalar(host[6], n=2)]
+    return host, dev
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_init_kernels_match_oracle(name):
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    for k, what in (("init_b", "init"), ("init_u", "u_init")):
+        buf = ctx.vec()
+        ctx.kernel(k, buf)
+        ref = o.grid(o.vec())
+        ref[...] = o._testcase(what, 0.0)
+        assert rel_err(ctx.get_vec(buf)[: o.N], ref.reshape(-1, 4)) <= (1e-6 if c.get("real") == "float" else 1e-13)
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_every_stage_kernel_matches_oracle(name):
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    host, dev = _fields(ctx, o, z, name)
+    nf = NUM_FIELDS[c["integrator"]]
+    sel = (lambda f: f if nf == 3 else [f[0], f[1]] + f[3:])
+    seq = rk_step(c["integrator"], c.get("hall", False), c.get("variable_u", False))
+    moved = 0.0
+    for _ in range(c["steps"]):
+        for k in seq:
+            ctx.run(k, o.cfg.nodes, *sel(dev))
+            o.run(k, o.cfg.nodes, *sel(host))
+            for i, (hd, dv) in enumerate(zip(host, dev)):
+                if i == 6:
+                    got = ctx.get_scalar(dv, n=2)
+                    np.testing.assert_allclose(got, hd, rtol=1e-15, atol=0, err_msg=k)
+                    continue
+                if nf == 2 and i == 2:
+                    continue
+                got = ctx.get_scalar(dv) if hd.ndim == 1 else ctx.get_vec(dv)
+                e = rel_err(got, hd)
+                assert e <= tol(c), (k, i, e)
+        moved = max(moved, rel_err(host[0], z[f"{name}/in_b"]))
+    assert moved > 1e-8, "the case must change the field"
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_fused_time_steps_match_oracle(name):
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    host, dev = _fields(ctx, o, z, name)
+    nf = NUM_FIELDS[c["integrator"]]
+    time_loop(o, c["integrator"], c.get("hall", False), c.get("variable_u", False), c["steps"],
+              host[0], host[1], host[2] if nf == 3 else None, host[3], host[4], host[5], host[6])
+    ctx.time_steps(*dev, c["steps"])
+    ctx.synchronize()
+    assert rel_err(ctx.get_vec(dev[0]), host[0]) <= tol(c)
+    assert rel_err(ctx.get_vec(dev[1]), host[1]) <= tol(c)
+    np.testing.assert_allclose(ctx.get_scalar(dev[6], n=2), host[6], rtol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["wave_6c_hall_hod_ck2n54", "rot_gauss_4c_ssprk33"])
+def test_fused_time_steps_are_bitwise_reproducible(name):
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    outs = []
+    for _ in range(2):
+        _, dev = _fields(ctx, o, z, name)
+        ctx.time_steps(*dev, 3)
+        outs.append(ctx.get_vec(dev[0]))
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("name", ["rot3d_2c_ck2n54", "wave_6c_hall_hod_ck2n54"])
+def test_fused_odd_and_even_step_counts(name):
+    # the fused 5-stage 2N step ping-pongs b1; odd counts copy the result back
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    for n in (1, 2, 3):
+        host, dev = _fields(ctx, o, z, name)
+        time_loop(o, c["integrator"], c.get("hall", False), False, n, host[0], host[1], None, host[3],
+                  host[4], host[5], host[6])
+        ctx.time_steps(*dev, n)
+        assert rel_err(ctx.get_vec(dev[0]), host[0]) <= TOL64, n
+
+
+@pytest.mark.parametrize("name", ["rot_gauss_4c_ssprk33", "rot3d_2c_ck2n54"])
+def test_host_array_call_runs_reference_time_loop(name):
+    # the MatCL-form call with host arrays (copy in, run the list, copy out)
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    hg, _ = _fields(ctx, o, z, name)
+    ho = [a.copy() for a in hg]
+    nf = NUM_FIELDS[c["integrator"]]
+    seq = rk_step(c["integrator"], False, False)
+    sel = (lambda f: f if nf == 3 else [f[0], f[1]] + f[3:])
+    for _ in range(c["steps"]):
+        ctx.run_host(seq, o.cfg.nodes, *sel(hg))
+        o.run_list(seq, o.cfg.nodes, *sel(ho))
+    assert rel_err(hg[0], ho[0]) <= TOL64
+    np.testing.assert_allclose(hg[6], ho[6], rtol=1e-15)
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_norms_match_oracle(name):
+    z, man = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    b = z[f"{name}/out_b"].astype(o.T)
+    t = float(z[f"{name}/out_time"][0])
+    res = ctx.results(ctx.vec(b), t, ctx.vec(), ctx.scalar())
+    ana = o.vec()
+    o.run("analytical_b", o.cfg.nodes, ana, np.array([t, t], dtype=o.T))
+    ref = norms(o, b.copy(), ana, o.scalar())
+    rt = 1e-5 if c.get("real") == "float" else 1e-11
+    for k in ("abs_err", "rel_err", "divergence_norm", "energy"):
+        assert abs(res[k] - ref[k]) <= rt * abs(ref[k]) + 1e-300, (k, res[k], ref[k])
+
+
+@pytest.mark.parametrize("name", sorted(CG_CASES))
+def test_clean_div_matches_oracle(name):
+    z, man = _golden()
+    c = CG_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    b = z[f"{name}/in_b"].copy()
+    ref = clean_div(o, b, c["max_iterations"], c["thr"], c["bnodes"])
+    db = ctx.vec(z[f"{name}/in_b"])
+    res = ctx.clean_div(db, c["max_iterations"], c["thr"], check=False)
+    assert res["iterations"] == ref["iterations"] == man[name]["iterations"]
+    assert abs(res["divergence_norm_initial"] - ref["initial_norm"]) <= 1e-12 * ref["initial_norm"]
+    assert abs(res["residual_norm2"] - ref["residual_norm2"]) <= 1e-6 * ref["residual_norm2"] + 1e-30
+    assert rel_err(ctx.get_vec(db), b) <= 1e-11
+
+
+@pytest.mark.parametrize("name", ["cg_4c_wsd0", "cg_2c_wsln"])
+def test_cg_kernels_through_reference_host_loop(name):
+    # the reference's host loop (clean_div.m) driving the per-kernel GPU entry points
+    z, man = _golden()
+    c = CG_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    r = host_runner(ctx, o.cfg.nodes)
+    bg = z[f"{name}/in_b"].copy()
+    bo = z[f"{name}/in_b"].copy()
+    rg = clean_div(r, bg, 10, c["thr"], c["bnodes"])
+    ro = clean_div(o, bo, 10, c["thr"], c["bnodes"])
+    assert rg["iterations"] == ro["iterations"]
+    np.testing.assert_allclose(rg["history"], ro["history"], rtol=1e-9)
+    assert rel_err(bg, bo) <= 1e-11
+
+
+def test_operators_match_oracle():
+    z, _ = _golden()
+    c = STEP_CASES["confined_6e_hall_fo_cfr"]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    b = z["confined_6e_hall_fo_cfr/out_b"]
+    n = o.cfg.nodes
+    for k in ("calc_div", "calc_curl"):
+        outd = ctx.scalar() if k == "calc_div" else ctx.vec()
+        ctx.run(k, n, ctx.vec(b), outd)
+        outh = o.scalar() if k == "calc_div" else o.vec()
+        o.run(k, n, b.copy(), outh)
+        got = ctx.get_scalar(outd) if k == "calc_div" else ctx.get_vec(outd)
+        assert rel_err(got, outh) <= 1e-12, k
+    s = b[:, 0].copy()
+    outd = ctx.vec()
+    ctx.run("calc_grad", n, ctx.scalar(s), outd)
+    outh = o.vec()
+    o.run("calc_grad", n, s, outh)
+    assert rel_err(ctx.get_vec(outd), outh) <= 1e-12
