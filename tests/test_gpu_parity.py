@@ -194,8 +194,11 @@ def test_norms_match_oracle(name):
     o.run("analytical_b", o.cfg.nodes, ana, np.array([t, t], dtype=o.T))
     ref = norms(o, b.copy(), ana, o.scalar())
     rt = 1e-5 if c.get("real") == "float" else 1e-11
+    # ||div B|| of a nearly divergence-free field is a cancellation: its absolute error is set
+    # by the rounding of B itself (~eps * |B| / dx), not by its own size
+    floor = {"divergence_norm": (1e-6 if c.get("real") == "float" else 1e-13) * ref["energy"] ** 0.5 / min(o.d)}
     for k in ("abs_err", "rel_err", "divergence_norm", "energy"):
-        assert abs(res[k] - ref[k]) <= rt * abs(ref[k]) + 1e-300, (k, res[k], ref[k])
+        assert abs(res[k] - ref[k]) <= rt * abs(ref[k]) + floor.get(k, 1e-300), (k, res[k], ref[k])
 
 
 @pytest.mark.parametrize("name", sorted(CG_CASES))
