@@ -147,6 +147,28 @@ ieq_status ieq_profile_step(ieq_ctx *ctx, void *b, void *b2, void *b3, void *cur
                             void *rho, void *time, int max_records, ieq_kernel_record *records,
                             int *n_records);
 
+/* ---------------------------------------------------------------- allocation-free dot */
+
+/* FP64 dot product sum_i a[i]*b[i] of two device arrays of n doubles, written to the device
+ * scalar result[0] on `stream` (a cudaStream_t; NULL = the default stream).  No counterpart
+ * in the reference: it exists for callers that cannot let a library allocate device memory --
+ * hosts whose device memory belongs to their own pool (a framework's caching allocator, a
+ * MATLAB mex working within a fixed budget) and time loops that must not allocate once they
+ * run.  It needs no context and calls no cudaMalloc, cudaFree or allocating library routine:
+ * its scratch (one FP64 partial per 2048 elements) is a fixed 32 KiB array in the library's
+ * device image, which every GPU that loads the library holds until the process exits.
+ *   - n may be at most IEQ_NOALLOC_DOT_MAX_ELEMENTS; larger n returns IEQ_ERR_SHAPE and
+ *     launches nothing.  NULL pointers return IEQ_ERR_ARG.
+ *   - The first call on a device looks up the scratch array's device address (once per
+ *     device, with that device current); make that first call before any stream capture.
+ *   - All calls share the one scratch array, which keeps the last call's partials.  Every
+ *     partial a call reads was written earlier in that call, so nothing needs clearing, but
+ *     calls that overlap on the GPU (other streams, other threads) race: order them.
+ *   - The sum is taken in a fixed order: repeated calls give bitwise identical results. */
+#define IEQ_NOALLOC_DOT_MAX_ELEMENTS 8388608
+ieq_status ieq_dot_product_noalloc(const double *a, const double *b, uint64_t n, double *result,
+                                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif
