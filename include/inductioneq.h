@@ -53,8 +53,7 @@ typedef struct ieq_ctx ieq_ctx;
  *   -DUSE_UIBJ_PRODUCT=1 ... -cl-mad-enable"); OpenCL compiler options are accepted and
  *   ignored.  Keys this library adds (all optional): -DIEQ_INTEGRATOR=<name of one of the
  *   six integrators> (host-side I_TI('time_integrator')), -DIEQ_VARIABLE_U=1
- *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>,
- *   -DIEQ_MIXED_CG=1 (FP64 CG vectors and reductions while REAL=float).
+ *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>.
  * kernel_paths: the kernel_path_list (compute_numerical_solution_setup.m:57-122).  Only
  *   the base names matter: the operator header ({2,4,6}thOrder[Extended].h) selects the SBP
  *   operator, "<testcase>.h" the testcase, artificial_dissipation.cl enables dissipation.
@@ -110,8 +109,10 @@ ieq_status ieq_time_steps(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB
 /* Divergence cleaning, matlab/+induction_eq/clean_div.m:36-79, device resident: CG on
  * (-Laplace) phi = div B over the interior, stopping when the unweighted squared
  * residual <= absolute_error_threshold^2 or after max_iterations, then B is projected.
- * The CG vectors and reductions are FP64 when REAL=double or -DIEQ_MIXED_CG=1.
- * Returns IEQ_ERR_NOT_CONVERGED (with B still projected) if the cap was hit. */
+ * The CG vectors (phi, r, u, Laplacian), the dot products, alpha/beta and the divergence and
+ * projection arithmetic are FP64 whatever REAL is (with REAL=float this is the precision
+ * form: FP32 state, FP64 solve).  Returns IEQ_ERR_NOT_CONVERGED (with B still projected)
+ * if the cap was hit. */
 ieq_status ieq_clean_div(ieq_ctx *ctx, void *b, int max_iterations,
                          double absolute_error_threshold, int *iterations,
                          double *residual_norm2, double *initial_divergence_norm);
@@ -136,16 +137,18 @@ ieq_status ieq_compute_results(ieq_ctx *ctx, const void *b, double t, void *work
 /* IEQ_ERR_NAN if any x/y/z component of the vector field is not finite, else IEQ_OK. */
 ieq_status ieq_check_finite(ieq_ctx *ctx, const void *vec_field);
 
-/* Profiling: one time step of ieq_time_steps launched without a graph, with a CUDA event
- * after every kernel; records[k] gets the kernel's label and device duration (ms), in
- * launch order (the kernel time MatCL returns, per kernel).  Synchronises. */
+/* Profiling (the per-kernel counterpart of the kernel time MatCL returns): every launch of
+ * one ieq_time_steps step is captured alone, `repeats` times back to back, into a CUDA graph
+ * and timed with events around the graph; records[k] gets the label and average device
+ * time (ms) of launch k, in launch order.  The fields are advanced by the repeated
+ * launches and hold no solution afterwards.  Synchronises. */
 typedef struct ieq_kernel_record {
   char name[40];
   double ms;
 } ieq_kernel_record;
 ieq_status ieq_profile_step(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
-                            void *rho, void *time, int max_records, ieq_kernel_record *records,
-                            int *n_records);
+                            void *rho, void *time, int repeats, int max_records,
+                            ieq_kernel_record *records, int *n_records);
 
 /* ---------------------------------------------------------------- allocation-free dot */
 

@@ -156,9 +156,9 @@ Forms flux_forms(const Settings &s) {
   return f;
 }
 
-template <typename R>
-StageArgs<R> stage_base(ieq_ctx *c, bool conv) {
-  StageArgs<R> a;
+template <typename R, typename F = AoS<R>>
+StageArgs<R, F> stage_base(ieq_ctx *c, bool conv) {
+  StageArgs<R, F> a;
   std::memset(&a, 0, sizeof(a));
   a.m = mesh_of(c);
   a.tab = tables<R>(c);
@@ -198,24 +198,24 @@ int diss_kind(const Settings &s) {
   return DISS_NONE;
 }
 
-template <typename R>
-void launch_stage_any(ieq_ctx *c, const StageArgs<R> &a) {
+template <typename R, typename F>
+void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
   const dim3 g = grid3(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2]), b = block3();
   const bool per = c->s.periodic, hall = c->s.hall;
   const int d = diss_kind(c->s);
   switch (c->op_id) {
-    case 0: launch_stage<R, 0>(a, per, hall, d, g, b, c->stream); break;
-    case 1: launch_stage<R, 1>(a, per, hall, d, g, b, c->stream); break;
-    case 2: launch_stage<R, 2>(a, per, hall, d, g, b, c->stream); break;
-    case 3: launch_stage<R, 3>(a, per, hall, d, g, b, c->stream); break;
-    case 4: launch_stage<R, 4>(a, per, hall, d, g, b, c->stream); break;
-    case 5: launch_stage<R, 5>(a, per, hall, d, g, b, c->stream); break;
+    case 0: launch_stage<R, F, 0>(a, per, hall, d, conv, g, b, c->stream); break;
+    case 1: launch_stage<R, F, 1>(a, per, hall, d, conv, g, b, c->stream); break;
+    case 2: launch_stage<R, F, 2>(a, per, hall, d, conv, g, b, c->stream); break;
+    case 3: launch_stage<R, F, 3>(a, per, hall, d, conv, g, b, c->stream); break;
+    case 4: launch_stage<R, F, 4>(a, per, hall, d, conv, g, b, c->stream); break;
+    case 5: launch_stage<R, F, 5>(a, per, hall, d, conv, g, b, c->stream); break;
   }
 }
 
-template <typename R>
-void launch_curl_any(ieq_ctx *c, const R4<R> *b, const R *rho, R4<R> *out) {
-  CurlArgs<R> a;
+template <typename R, typename F>
+void launch_curl_any(ieq_ctx *c, F b, const R *rho, F out) {
+  CurlArgs<R, F> a;
   std::memset(&a, 0, sizeof(a));
   a.m = mesh_of(c);
   a.b = b;
@@ -225,16 +225,19 @@ void launch_curl_any(ieq_ctx *c, const R4<R> *b, const R *rho, R4<R> *out) {
   const SbpOperator &op = c->op;
   const int RI = op.order / 2, C0 = (op.sw - 1) / 2;
   for (int o = -RI; o <= RI; ++o) a.Dint[o + RI] = (R)op.D.at(op.nb, C0 + o);
-  for (int ax = 0; ax < 3; ++ax) a.dR[ax] = (R)c->s.d[ax];
+  for (int ax = 0; ax < 3; ++ax) {
+    a.dR[ax] = (R)c->s.d[ax];
+    a.inv_d[ax] = (R)(1.0 / c->s.d[ax]);
+  }
   const dim3 g = grid3(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2]), bl = block3();
   const bool per = c->s.periodic;
   switch (c->op_id) {
-    case 0: launch_curl<R, 0>(a, per, g, bl, c->stream); break;
-    case 1: launch_curl<R, 1>(a, per, g, bl, c->stream); break;
-    case 2: launch_curl<R, 2>(a, per, g, bl, c->stream); break;
-    case 3: launch_curl<R, 3>(a, per, g, bl, c->stream); break;
-    case 4: launch_curl<R, 4>(a, per, g, bl, c->stream); break;
-    case 5: launch_curl<R, 5>(a, per, g, bl, c->stream); break;
+    case 0: launch_curl<R, F, 0>(a, per, g, bl, c->stream); break;
+    case 1: launch_curl<R, F, 1>(a, per, g, bl, c->stream); break;
+    case 2: launch_curl<R, F, 2>(a, per, g, bl, c->stream); break;
+    case 3: launch_curl<R, F, 3>(a, per, g, bl, c->stream); break;
+    case 4: launch_curl<R, F, 4>(a, per, g, bl, c->stream); break;
+    case 5: launch_curl<R, F, 5>(a, per, g, bl, c->stream); break;
   }
 }
 
@@ -362,7 +365,7 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
   if (nm == "init_b" || nm == "init_u" || nm == "init_rho" || nm == "analytical_b") {
     if ((st = need(nm == "analytical_b" ? 2 : 1)) != IEQ_OK) return st;
     const int kind = nm == "init_b" ? INIT_B : nm == "init_u" ? INIT_U : nm == "init_rho" ? INIT_RHO : ANALYTICAL_B;
-    k_init<R><<<grid, blk, 0, c->stream>>>(m, c->s.testcase, kind, (R4<R> *)args[0], (R *)args[0],
+    k_init<R><<<grid, blk, 0, c->stream>>>(m, c->s.testcase, kind, (R *)args[0], 0, (R *)args[0],
                                            nargs > 1 ? (const R *)args[1] : nullptr);
     IEQ_LAUNCHED(c);
     return IEQ_OK;
@@ -379,7 +382,7 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
   if (nm == "calc_div" || nm == "calc_grad" || nm == "calc_curl") {
     if ((st = need(2)) != IEQ_OK) return st;
     if (nm == "calc_curl") {
-      launch_curl_any<R>(c, (const R4<R> *)args[0], nullptr, (R4<R> *)args[1]);
+      launch_curl_any<R, AoS<R>>(c, AoS<R>{(R4<R> *)args[0]}, nullptr, AoS<R>{(R4<R> *)args[1]});
       IEQ_LAUNCHED(c);
       return IEQ_OK;
     }
@@ -448,29 +451,30 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
   for (int i = 0; i < nargs; ++i)
     if (!args[i]) return fail(c, IEQ_ERR_ARG, nm + ": null argument");
   auto vec = [&](int k) { return (R4<R> *)f.b[k]; };
+  auto fv = [&](int k) { return AoS<R>{(R4<R> *)f.b[k]}; };
   if (nm == "calc_time_2_args" || nm == "calc_time_3_args") return launch_time<R>(c, f.time, 2, (R)0);
   if (nm == "calc_u_2_args" || nm == "calc_u_3_args") {
-    k_init<R><<<grid, blk, 0, c->stream>>>(m, c->s.testcase, CALC_U, (R4<R> *)f.u, nullptr, (const R *)f.time);
+    k_init<R><<<grid, blk, 0, c->stream>>>(m, c->s.testcase, CALC_U, (R *)f.u, 0, nullptr, (const R *)f.time);
     IEQ_LAUNCHED(c);
     return IEQ_OK;
   }
   if (nm.rfind("calc_curlB_rho_", 0) == 0) {
     const int k = nm[15] - '0';
-    launch_curl_any<R>(c, vec(k), (const R *)f.rho, (R4<R> *)f.cb);
+    launch_curl_any<R, AoS<R>>(c, fv(k), (const R *)f.rho, AoS<R>{(R4<R> *)f.cb});
     IEQ_LAUNCHED(c);
     return IEQ_OK;
   }
   if (c->s.uibj < 0 || c->s.source < 0 || c->s.ujbi < 0)
     return fail(c, IEQ_ERR_SETTINGS, "no discretization of the volume terms specified (USE_UIBJ_*, USE_SOURCE_*, USE_UJBI_*)");
   StageArgs<R> a = stage_base<R>(c, true);
-  a.J = (const R4<R> *)f.cb;
-  a.u = (const R4<R> *)f.u;
+  a.J = AoS<R>{(R4<R> *)f.cb};
+  a.u = AoS<R>{(R4<R> *)f.u};
   a.time = (R *)f.time;
-  auto stage = [&](int src, int mode, R4<R> *out) {
-    a.bk = vec(src);
+  auto stage = [&](int src, int mode, AoS<R> out) {
+    a.bk = fv(src);
     a.mode = mode;
     a.out = out;
-    launch_stage_any<R>(c, a);
+    launch_stage_any<R, AoS<R>>(c, a);
   };
   auto pointwise = [&](int mode, R4<R> *P, R4<R> *Q, R4<R> *D, R c1, R c2, int tkind, R tK) -> ieq_status {
     const int nb = (int)((n + 255) / 256);
@@ -479,16 +483,16 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
     return IEQ_OK;
   };
   // SSPRK33 (224-303)
-  if (nm == "SSPRK33_1") { a.X = vec(1); a.h = DT; stage(1, EP_X_PLUS_HF, vec(2)); IEQ_LAUNCHED(c); return IEQ_OK; }
+  if (nm == "SSPRK33_1") { a.X = fv(1); a.h = DT; stage(1, EP_X_PLUS_HF, fv(2)); IEQ_LAUNCHED(c); return IEQ_OK; }
   if (nm == "SSPRK33_2a") return launch_time<R>(c, f.time, 1, DT);
   if (nm == "SSPRK33_2b") {
-    a.X = vec(1); a.Y = vec(2); a.p = (R)0.75; a.q = (R)0.25; a.h = DT;
-    stage(2, EP_PX_QYHF, vec(3)); IEQ_LAUNCHED(c); return IEQ_OK;
+    a.X = fv(1); a.Y = fv(2); a.p = (R)0.75; a.q = (R)0.25; a.h = DT;
+    stage(2, EP_PX_QYHF, fv(3)); IEQ_LAUNCHED(c); return IEQ_OK;
   }
   if (nm == "SSPRK33_3a") return launch_time<R>(c, f.time, 1, (R)(0.5 * c->s.dt));
   if (nm == "SSPRK33_3b") {
-    a.X = vec(1); a.Y = vec(3); a.p = (R)(1.0 / 3.0); a.q = (R)(2.0 / 3.0); a.h = DT;
-    stage(3, EP_PX_QYHF, vec(1)); IEQ_LAUNCHED(c); return IEQ_OK;
+    a.X = fv(1); a.Y = fv(3); a.p = (R)(1.0 / 3.0); a.q = (R)(2.0 / 3.0); a.h = DT;
+    stage(3, EP_PX_QYHF, fv(1)); IEQ_LAUNCHED(c); return IEQ_OK;
   }
   // SSPRK104 (315-621)
   if (nm.rfind("SSPRK104_", 0) == 0) {
@@ -504,8 +508,8 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
     }
     const std::string s2 = tag.substr(0, 2);
     if (s2 == "11") {
-      a.X = vec(3); a.Y = vec(2); a.p = (R)1; a.q = (R)0.6; a.h = h;
-      stage(2, EP_PX_QYHF, vec(1)); IEQ_LAUNCHED(c); return IEQ_OK;
+      a.X = fv(3); a.Y = fv(2); a.p = (R)1; a.q = (R)0.6; a.h = h;
+      stage(2, EP_PX_QYHF, fv(1)); IEQ_LAUNCHED(c); return IEQ_OK;
     }
     int src = 0, dst = 0;
     if (s2 == "01") { src = 1; dst = 2; } else if (s2 == "02") { src = 2; dst = 3; }
@@ -514,8 +518,8 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
     else if (s2 == "08") { src = 1; dst = 2; } else if (s2 == "09") { src = 2; dst = 1; }
     else if (s2 == "10") { src = 1; dst = 2; }
     else return fail(c, IEQ_ERR_UNKNOWN_KERNEL, "unknown kernel " + nm);
-    a.X = vec(src); a.h = h;
-    stage(src, EP_X_PLUS_HF, vec(dst)); IEQ_LAUNCHED(c); return IEQ_OK;
+    a.X = fv(src); a.h = h;
+    stage(src, EP_X_PLUS_HF, fv(dst)); IEQ_LAUNCHED(c); return IEQ_OK;
   }
   // 2R schemes (630-1007): the third field is db
   const bool kcl = nm.rfind("KennedyCarpenterLewis2R54C_", 0) == 0;
@@ -529,13 +533,13 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
     const int *src = kcl ? kKCLsrc : kCFRsrc;
     if (sidx == last && tag.size() == 1) {
       // b1 = b1 + coef_B*(REAL)(DT) * DB(b2)
-      a.X = vec(1); a.h = (R)tab[sidx][1] * DT;
-      stage(2, EP_X_PLUS_HF, vec(1)); IEQ_LAUNCHED(c); return IEQ_OK;
+      a.X = fv(1); a.h = (R)tab[sidx][1] * DT;
+      stage(2, EP_X_PLUS_HF, fv(1)); IEQ_LAUNCHED(c); return IEQ_OK;
     }
     if (tag.size() != 2) return fail(c, IEQ_ERR_UNKNOWN_KERNEL, "unknown kernel " + nm);
     if (tag[1] == 'a') {
       a.h = DT;
-      stage(src[sidx], EP_HF, vec(3)); IEQ_LAUNCHED(c); return IEQ_OK;
+      stage(src[sidx], EP_HF, fv(3)); IEQ_LAUNCHED(c); return IEQ_OK;
     }
     const R A = (R)tab[sidx][0], Bc = (R)tab[sidx][1];
     const double C = tab[sidx][2];
@@ -560,8 +564,8 @@ ieq_status run_one(ieq_ctx *c, const char *name, const uint32_t *g, void *const 
     const double *Atab = ck ? kCK_A : kTD_A, *Btab = ck ? kCK_B : kTD_B, *Ctab = ck ? kCK_C : kTD_C;
     if (tag[1] == 'a') {
       a.h = DT;
-      if (sidx == 0) stage(1, EP_HF, vec(2));
-      else { a.X = vec(2); a.A = (R)Atab[sidx]; stage(1, EP_AX_HF, vec(2)); }
+      if (sidx == 0) stage(1, EP_HF, fv(2));
+      else { a.X = fv(2); a.A = (R)Atab[sidx]; stage(1, EP_AX_HF, fv(2)); }
       IEQ_LAUNCHED(c);
       return IEQ_OK;
     }
@@ -682,7 +686,7 @@ void ieq_destroy(ieq_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   void *own[] = {c->d_tables, c->d_rows_r, c->d_rows_d, c->d_lap_r, c->d_lap_d, c->d_wnorm, c->d_partials,
                  c->d_partials2, c->d_total, c->d_counter, c->d_flag, c->d_cg, c->d_cg_vec, c->d_cg_hist,
-                 c->d_pingpong};
+                 c->d_pingpong, c->d_soa};
   for (void *p : own)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);

@@ -84,7 +84,8 @@ struct ieq_ctx {
   double *d_cg_vec = nullptr;      // FP64 CG vectors: div, phi, r, u, lap (5 x n_pad)
   double *d_cg_hist = nullptr;
   int cg_hist_len = 0;
-  void *d_pingpong = nullptr;      // second b1 buffer of the fused 2N step
+  void *d_pingpong = nullptr;      // (unused)
+  void *d_soa = nullptr;           // structure-of-arrays state of the fused time stepping
   std::set<void *> allocs;
   // fused time-step graphs keyed by the argument pointers
   struct GraphEntry {
@@ -92,6 +93,9 @@ struct ieq_ctx {
   };
   std::map<std::vector<uintptr_t>, GraphEntry> graphs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // per-kernel event records of ieq_profile_step (label, event after the launch)
-  std::vector<std::pair<std::string, cudaEvent_t>> *recorder = nullptr;
+  // ieq_profile_step: labels of the step's launches, and a gate that lets only the
+  // launch with index gate_target through (-1: all launches, -2: none)
+  std::vector<std::string> *labels = nullptr;
+  int gate_target = -1;
+  int gate_count = 0;
 };

@@ -10,19 +10,31 @@ namespace ieq {
 enum InitKind : int { INIT_B = 0, INIT_U = 1, INIT_RHO = 2, ANALYTICAL_B = 3, CALC_U = 4 };
 
 // kernel_init.cl:3-48 and kernel_time_integrator.cl:93-125 (u = u_analytical(time[1]))
+// vout: REAL4 AoS (vstride = 0) or SoA with component stride vstride
 template <typename R>
-__global__ void k_init(Mesh m, int tc, int kind, R4<R> *vout, R *sout, const R *time) {
+__device__ __forceinline__ void st_any(R *base, long long vstride, long long idx, V3<R> v) {
+  if (vstride == 0) {
+    st3(reinterpret_cast<R4<R> *>(base) + idx, v);
+  } else {
+    base[idx] = v.x;
+    base[idx + vstride] = v.y;
+    base[idx + 2 * vstride] = v.z;
+  }
+}
+
+template <typename R>
+__global__ void k_init(Mesh m, int tc, int kind, R *vout, long long vstride, R *sout, const R *time) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
   if (ix >= m.nx || iy >= m.ny || iz >= m.nz) return;
   const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
   switch (kind) {
-    case INIT_B: st3(vout + idx, b_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
-    case INIT_U: st3(vout + idx, u_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
+    case INIT_B: st_any(vout, vstride, idx, b_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
+    case INIT_U: st_any(vout, vstride, idx, u_analytical<R>(tc, m, ix, iy, iz, (R)0)); break;
     case INIT_RHO: sout[idx] = (R)1; break;
-    case ANALYTICAL_B: st3(vout + idx, b_analytical<R>(tc, m, ix, iy, iz, time[0])); break;
-    case CALC_U: st3(vout + idx, u_analytical<R>(tc, m, ix, iy, iz, time[1])); break;
+    case ANALYTICAL_B: st_any(vout, vstride, idx, b_analytical<R>(tc, m, ix, iy, iz, time[0])); break;
+    case CALC_U: st_any(vout, vstride, idx, u_analytical<R>(tc, m, ix, iy, iz, time[1])); break;
   }
 }
 

@@ -1,14 +1,14 @@
-// stage_inst.cuh -- instantiates the stage and curl kernels for one (REAL, operator) pair.
-// Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so the instantiations
-// compile in parallel.
+// stage_inst.cuh -- instantiates the stage and curl kernels for one (REAL, operator) pair in
+// both field layouts.  Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so
+// the instantiations compile in parallel.
 #include "stage_kernel.cuh"
 
 namespace ieq {
 
-template <>
-void launch_stage<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R> &a, bool per, bool hall, int diss, dim3 grid,
-                                 dim3 block, cudaStream_t s) {
-#define IEQ_L(P, H, D) k_stage<IEQ_R, IEQ_OP, P, H, D><<<grid, block, 0, s>>>(a)
+template <typename F, int C>
+static void launch_stage_layout(const StageArgs<IEQ_R, F> &a, bool per, bool hall, int diss, dim3 grid,
+                                dim3 block, cudaStream_t s) {
+#define IEQ_L(P, H, D) k_stage<IEQ_R, F, IEQ_OP, P, H, D, C><<<grid, block, 0, s>>>(a)
   if (per) {
     if (hall) {
       if (diss == DISS_NONE) IEQ_L(true, true, DISS_NONE);
@@ -33,10 +33,32 @@ void launch_stage<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R> &a, bool per, bool hall,
 #undef IEQ_L
 }
 
+// the per-kernel entry points (AoS) decide the convection switch at run time; the fused
+// path (SoA) knows it before capturing its graph
 template <>
-void launch_curl<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R> &a, bool per, dim3 grid, dim3 block, cudaStream_t s) {
-  if (per) k_curl_rho<IEQ_R, IEQ_OP, true><<<grid, block, 0, s>>>(a);
-  else k_curl_rho<IEQ_R, IEQ_OP, false><<<grid, block, 0, s>>>(a);
+void launch_stage<IEQ_R, AoS<IEQ_R>, IEQ_OP>(const StageArgs<IEQ_R, AoS<IEQ_R>> &a, bool per, bool hall, int diss,
+                                             int conv, dim3 grid, dim3 block, cudaStream_t s) {
+  (void)conv;
+  launch_stage_layout<AoS<IEQ_R>, -1>(a, per, hall, diss, grid, block, s);
+}
+template <>
+void launch_stage<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, int diss,
+                                             int conv, dim3 grid, dim3 block, cudaStream_t s) {
+  if (conv == 0) launch_stage_layout<SoA<IEQ_R>, 0>(a, per, hall, diss, grid, block, s);
+  else launch_stage_layout<SoA<IEQ_R>, 1>(a, per, hall, diss, grid, block, s);
+}
+
+template <>
+void launch_curl<IEQ_R, AoS<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, AoS<IEQ_R>> &a, bool per, dim3 grid, dim3 block,
+                                            cudaStream_t s) {
+  if (per) k_curl_rho<IEQ_R, AoS<IEQ_R>, IEQ_OP, true><<<grid, block, 0, s>>>(a);
+  else k_curl_rho<IEQ_R, AoS<IEQ_R>, IEQ_OP, false><<<grid, block, 0, s>>>(a);
+}
+template <>
+void launch_curl<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, dim3 grid, dim3 block,
+                                            cudaStream_t s) {
+  if (per) k_curl_rho<IEQ_R, SoA<IEQ_R>, IEQ_OP, true><<<grid, block, 0, s>>>(a);
+  else k_curl_rho<IEQ_R, SoA<IEQ_R>, IEQ_OP, false><<<grid, block, 0, s>>>(a);
 }
 
 }  // namespace ieq

@@ -23,6 +23,39 @@
 
 namespace ieq {
 
+// ---- field layouts: REAL4 array-of-structs (the reference's layout, used by the per-kernel
+// entry points) and structure-of-arrays (x, y, z planes of one allocation, component stride s;
+// used by the fused time stepping: a warp's neighbour load is 256 contiguous bytes).
+template <typename R>
+struct AoS {
+  R4<R> *p;
+};
+template <typename R>
+struct SoA {
+  R *p;
+  long long s;
+};
+template <typename R>
+__device__ __forceinline__ V3<R> ldf(const AoS<R> &f, long long j) { return ld3(f.p + j); }
+template <typename R>
+__device__ __forceinline__ V3<R> ldf(const SoA<R> &f, long long j) {
+  return {__ldg(f.p + j), __ldg(f.p + j + f.s), __ldg(f.p + j + 2 * f.s)};
+}
+template <typename R>
+__device__ __forceinline__ V3<R> ldf_plain(const AoS<R> &f, long long j) { return ld3_plain(f.p + j); }
+template <typename R>
+__device__ __forceinline__ V3<R> ldf_plain(const SoA<R> &f, long long j) {
+  return {f.p[j], f.p[j + f.s], f.p[j + 2 * f.s]};
+}
+template <typename R>
+__device__ __forceinline__ void stf(const AoS<R> &f, long long j, V3<R> v) { st3(f.p + j, v); }
+template <typename R>
+__device__ __forceinline__ void stf(const SoA<R> &f, long long j, V3<R> v) {
+  f.p[j] = v.x;
+  f.p[j + f.s] = v.y;
+  f.p[j + 2 * f.s] = v.z;
+}
+
 enum EpilogueMode : int {
   EP_X_PLUS_HF = 0,   // out = X + h*F                 SSPRK33_1, SSPRK104, KCL_5, CFR_6
   EP_PX_QYHF = 1,     // out = p*X + q*(Y + h*F)       SSPRK33_2b/3b, SSPRK104_11b
@@ -40,14 +73,14 @@ enum TimePost : int {
 
 enum DissKind : int { DISS_NONE = 0, DISS_HO = 1, DISS_FO_OR_AD = 2 };
 
-template <typename R>
+template <typename R, typename F = AoS<R>>
 struct StageArgs {
   Mesh m;
-  const R4<R> *bk;      // field the derivative is taken of
-  const R4<R> *J;       // curl(B)/rho (Hall)
-  const R4<R> *u;
-  const R4<R> *X, *Y, *Z;
-  R4<R> *out, *out2;
+  F bk;                 // field the derivative is taken of
+  F J;                  // curl(B)/rho (Hall)
+  F u;
+  F X, Y, Z;
+  F out, out2;
   const Tables<R> *tab;
   R *time;
   unsigned *counter;    // last-block ticket for the time post-update
@@ -90,12 +123,14 @@ struct AxisSums {
   V3<R> SuiBa, SU, SB, SuaB, SH, SHo;
 };
 
-template <typename R, bool HALL, bool HOD>
-__device__ __forceinline__ void accumulate(AxisSums<R> &s, const StageArgs<R> &a, int conv, int axis, R cD, R cH,
+// CHK: test the coefficients for zero at run time (boundary rows); the interior rows call
+// this with compile-time knowledge instead (only the centre derivative coefficient is zero)
+template <typename R, typename F, bool HALL, bool HOD, bool CHK>
+__device__ __forceinline__ void accumulate(AxisSums<R> &s, const StageArgs<R, F> &a, int conv, int axis, R cD, R cH,
                                            long long j) {
-  const V3<R> B = ld3(a.bk + j);
-  if (conv && cD != (R)0) {
-    const V3<R> U = ld3(a.u + j);
+  const V3<R> B = ldf(a.bk, j);
+  if (conv && (!CHK || cD != (R)0)) {
+    const V3<R> U = ldf(a.u, j);
     const R Ba = axis == 0 ? B.x : (axis == 1 ? B.y : B.z);
     const R Ua = axis == 0 ? U.x : (axis == 1 ? U.y : U.z);
     if (a.need & 1) {
@@ -107,24 +142,24 @@ __device__ __forceinline__ void accumulate(AxisSums<R> &s, const StageArgs<R> &a
       s.SuaB.x += cD * (Ua * B.x); s.SuaB.y += cD * (Ua * B.y); s.SuaB.z += cD * (Ua * B.z);
     }
   }
-  if (HALL && cD != (R)0) {
-    // Hall_volume: D[J_a B - J B_a]
-    const V3<R> Jk = ld3(a.J + j);
+  if (HALL && (!CHK || cD != (R)0)) {
+    // Hall_volume: D[J_a B - J B_a]; the a-component is J_a B_a - J_a B_a = 0
+    const V3<R> Jk = ldf(a.J, j);
     const R Ja = axis == 0 ? Jk.x : (axis == 1 ? Jk.y : Jk.z);
     const R Ba = axis == 0 ? B.x : (axis == 1 ? B.y : B.z);
-    s.SH.x += cD * (Ja * B.x - Jk.x * Ba);
-    s.SH.y += cD * (Ja * B.y - Jk.y * Ba);
-    s.SH.z += cD * (Ja * B.z - Jk.z * Ba);
+    if (axis != 0) s.SH.x += cD * (Ja * B.x - Jk.x * Ba);
+    if (axis != 1) s.SH.y += cD * (Ja * B.y - Jk.y * Ba);
+    if (axis != 2) s.SH.z += cD * (Ja * B.z - Jk.z * Ba);
   }
-  if (HOD && cH != (R)0) {
+  if (HOD && (!CHK || cH != (R)0)) {
     s.SHo.x += cH * B.x; s.SHo.y += cH * B.y; s.SHo.z += cH * B.z;
   }
 }
 
 // first-order / adaptive dissipation (artificial_dissipation.cl:36-160), evaluated as in
 // the reference per stencil point; used only by the DISS_FO_OR_AD instantiation.
-template <typename R, int OP, bool PER>
-__device__ V3<R> fo_ad_dissipation(const StageArgs<R> &a, const int ii[3], const int nn[3],
+template <typename R, typename F, int OP, bool PER>
+__device__ V3<R> fo_ad_dissipation(const StageArgs<R, F> &a, const int ii[3], const int nn[3],
                                    const long long st[3], long long idx, V3<R> Bm, V3<R> um) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH;
   V3<R> acc = {0, 0, 0};
@@ -147,8 +182,8 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R> &a, const int ii[3], const
       const int o = c - C0;
       const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
       const R cd = fabs(a.tab->D[row][c]);
-      const V3<R> Bk = ld3(a.bk + j);
-      const V3<R> uk = ld3(a.u + j);
+      const V3<R> Bk = ldf(a.bk, j);
+      const V3<R> uk = ldf(a.u, j);
       V3<R> sg = {fmax(fabs(uk.x), fabs(um.x)), fmax(fabs(uk.y), fabs(um.y)), fmax(fabs(uk.z), fabs(um.z))};
       if (adaptive) {
         const unsigned k = (unsigned)(o < 0 ? -o : o);
@@ -170,14 +205,14 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R> &a, const int ii[3], const
         const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
         const long long j1 = idx + (long long)(nbr<PER>(ii[ax], term + WH - 1, nn[ax]) - ii[ax]) * st[ax];
         const long long j2 = idx + (long long)(nbr<PER>(ii[ax], term + WH - 2, nn[ax]) - ii[ax]) * st[ax];
-        const V3<R> b1 = ld3(a.bk + j1), b2 = ld3(a.bk + j2), u1 = ld3(a.u + j1), u2 = ld3(a.u + j2);
+        const V3<R> b1 = ldf(a.bk, j1), b2 = ldf(a.bk, j2), u1 = ldf(a.u, j1), u2 = ldf(a.u, j2);
         // diff_HOD (artificial_dissipation.h:58-101) for this start offset
         const R sgn = (Op<OP>::ORDER / 2 + 1) % 2 ? (R)-1 : (R)1;
         V3<R> hod = {0, 0, 0};
         for (int i = 0; i < WH; ++i) {
           const R coef = ((a.tab->Minv[row] * a.tab->DHO[row][term + WH - 1]) * a.tab->DHO[NB][i]) * sgn;
           const long long j = idx + (long long)(nbr<PER>(ii[ax], i + term, nn[ax]) - ii[ax]) * st[ax];
-          const V3<R> Bk = ld3(a.bk + j);
+          const V3<R> Bk = ldf(a.bk, j);
           hod.x += coef * Bk.x; hod.y += coef * Bk.y; hod.z += coef * Bk.z;
         }
         acc.x += (((R)1 - kap(1, a.dR[ax], b1.x, b2.x, u1.x, u2.x)) * a.hod_factor) * hod.x;
@@ -189,8 +224,8 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R> &a, const int ii[3], const
   return acc;
 }
 
-template <typename R, int OP, bool PER, bool HALL, int DISS>
-__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R> a) {
+template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV = -1>
+__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R, F> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH;
   constexpr int RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
@@ -205,10 +240,10 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
     const int ii[3] = {ix, iy, iz};
     const int nn[3] = {nx, ny, nz};
     const long long st[3] = {1, nx, (long long)nx * ny};
-    const int conv = a.conv_flag ? *a.conv_flag : a.conv;
-    const V3<R> Bm = ld3(a.bk + idx);
+    const int conv = CONV >= 0 ? CONV : (a.conv_flag ? *a.conv_flag : a.conv);
+    const V3<R> Bm = ldf(a.bk, idx);
     V3<R> um = {0, 0, 0};
-    if (conv) um = ld3(a.u + idx);
+    if (conv) um = ldf(a.u, idx);
     V3<R> db = {0, 0, 0};
     V3<R> hod = {0, 0, 0};
 #pragma unroll
@@ -216,16 +251,21 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
       AxisSums<R> s{};
       const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
       if (row == NB) {
+        // periodic neighbours wrap only within RI of the ends of the axis
+        const bool wrap = PER && (ii[ax] < RI || ii[ax] >= nn[ax] - RI);
 #pragma unroll
         for (int o = -RI; o <= RI; ++o) {
           const R cD = a.Dint[o + RI];
           const R cH = a.Hint[o + RI];
           long long j = idx;
           if (o != 0) {
-            if (PER) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+            if (wrap) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
             else j = idx + (long long)o * st[ax];
+            accumulate<R, F, HALL, HOD, false>(s, a, conv, ax, cD, cH, j);
+          } else if (HOD) {
+            // the interior derivative rows have a zero centre
+            accumulate<R, F, false, HOD, false>(s, a, 0, ax, cD, cH, j);
           }
-          accumulate<R, HALL, HOD>(s, a, conv, ax, cD, cH, j);
         }
       } else {
         for (int o = -RB; o <= RB; ++o) {
@@ -233,7 +273,7 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
           const R cH = (HOD && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
           if (cD == (R)0 && cH == (R)0) continue;
           const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
-          accumulate<R, HALL, HOD>(s, a, conv, ax, cD, cH, j);
+          accumulate<R, F, HALL, HOD, true>(s, a, conv, ax, cD, cH, j);
         }
       }
       if (conv) {
@@ -268,7 +308,7 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
       if (face) {
         if (HALL) {
           // induction_Eq_surface.cl:35-81 (outflow, directional do-nothing)
-          const V3<R> Jm = ld3(a.J + idx);
+          const V3<R> Jm = ldf(a.J, idx);
           const V3<R> tv = {(R)0.5 * um.x - Jm.x, (R)0.5 * um.y - Jm.y, (R)0.5 * um.z - Jm.z};
           for (int ax = 0; ax < 3; ++ax) {
             const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
@@ -304,45 +344,45 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
       db.z += a.hod_factor * hod.z;
     }
     if (DISS == DISS_FO_OR_AD) {
-      const V3<R> ds = fo_ad_dissipation<R, OP, PER>(a, ii, nn, st, idx, Bm, um);
+      const V3<R> ds = fo_ad_dissipation<R, F, OP, PER>(a, ii, nn, st, idx, Bm, um);
       db.x += ds.x; db.y += ds.y; db.z += ds.z;
     }
     // ---- stage update
     V3<R> r;
     switch (a.mode) {
       case EP_X_PLUS_HF: {
-        const V3<R> X = ld3_plain(a.X + idx);
+        const V3<R> X = ldf_plain(a.X, idx);
         r = {X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
-        st3(a.out + idx, r);
+        stf(a.out, idx, r);
         break;
       }
       case EP_PX_QYHF: {
-        const V3<R> X = ld3_plain(a.X + idx), Y = ld3_plain(a.Y + idx);
+        const V3<R> X = ldf_plain(a.X, idx), Y = ldf_plain(a.Y, idx);
         r = {a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
              a.p * X.z + a.q * (Y.z + a.h * db.z)};
-        st3(a.out + idx, r);
+        stf(a.out, idx, r);
         break;
       }
       case EP_HF:
-        st3(a.out + idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
+        stf(a.out, idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
         break;
       case EP_AX_HF: {
-        const V3<R> X = ld3_plain(a.X + idx);
-        st3(a.out + idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
+        const V3<R> X = ldf_plain(a.X, idx);
+        stf(a.out, idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
         break;
       }
       case EP_2N_FUSED:
       case EP_2N_FUSED_FIRST: {
         V3<R> t;
         if (a.mode == EP_2N_FUSED) {
-          const V3<R> X = ld3_plain(a.X + idx);
+          const V3<R> X = ldf_plain(a.X, idx);
           t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
         } else {
           t = {a.h * db.x, a.h * db.y, a.h * db.z};
         }
-        st3(a.out + idx, t);
-        const V3<R> Z = ld3_plain(a.Z + idx);
-        st3(a.out2 + idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
+        stf(a.out, idx, t);
+        const V3<R> Z = ldf_plain(a.Z, idx);
+        stf(a.out2, idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
         break;
       }
     }
@@ -371,19 +411,42 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
 
 // curl(b)/rho (kernel_time_integrator.cl:136-208 via SBP_operator.cl:126-135), with the
 // same interior/boundary row split; diff_* divide by (REAL)DX as the reference does.
-template <typename R>
+template <typename R, typename F = AoS<R>>
 struct CurlArgs {
   Mesh m;
-  const R4<R> *b;
+  F b;
   const R *rho;       // nullptr: plain curl (kernel_operator.cl:158 calc_curl)
-  R4<R> *out;
+  F out;
   const Tables<R> *tab;
   R dR[3];
+  R inv_d[3];   // (REAL)(1.0/DX) ...
   R Dint[7];
 };
 
-template <typename R, int OP, bool PER>
-__global__ void __launch_bounds__(256) k_curl_rho(const __grid_constant__ CurlArgs<R> a) {
+template <typename R, typename F>
+__device__ __forceinline__ R ldc(const F &f, long long j, int comp);
+template <>
+__device__ __forceinline__ double ldc<double, SoA<double>>(const SoA<double> &f, long long j, int comp) {
+  return __ldg(f.p + j + comp * f.s);
+}
+template <>
+__device__ __forceinline__ float ldc<float, SoA<float>>(const SoA<float> &f, long long j, int comp) {
+  return __ldg(f.p + j + comp * f.s);
+}
+template <>
+__device__ __forceinline__ double ldc<double, AoS<double>>(const AoS<double> &f, long long j, int comp) {
+  return __ldg(reinterpret_cast<const double *>(f.p + j) + comp);
+}
+template <>
+__device__ __forceinline__ float ldc<float, AoS<float>>(const AoS<float> &f, long long j, int comp) {
+  return __ldg(reinterpret_cast<const float *>(f.p + j) + comp);
+}
+
+// curl(b)/rho.  Each axis contributes the derivatives of the two components orthogonal to
+// it; the derivative rows are multiplied by (REAL)(1/DX) and the curl by 1/rho (within one
+// rounding of the reference's divisions).
+template <typename R, typename F, int OP, bool PER>
+__global__ void __launch_bounds__(256) k_curl_rho(const __grid_constant__ CurlArgs<R, F> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -393,46 +456,67 @@ __global__ void __launch_bounds__(256) k_curl_rho(const __grid_constant__ CurlAr
   const int ii[3] = {ix, iy, iz};
   const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
   const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
-  V3<R> g[3];
+  R g[3][3];   // g[axis][component]
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
-    V3<R> v = {0, 0, 0};
+    const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+    R v1 = 0, v2 = 0;
     const int row = PER ? NB : sbp_row(ii[ax], nn[ax], NB);
     if (row == NB) {
+      const bool wrap = PER && (ii[ax] < RI || ii[ax] >= nn[ax] - RI);
 #pragma unroll
       for (int o = -RI; o <= RI; ++o) {
-        const R c = a.Dint[o + RI];
         if (o == 0) continue;   // the interior row has a zero centre
+        const R c = a.Dint[o + RI];
         long long j;
-        if (PER) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
+        if (wrap) j = idx + (long long)(nbr<true>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
         else j = idx + (long long)o * st[ax];
-        const V3<R> B = ld3(a.b + j);
-        v.x += c * B.x; v.y += c * B.y; v.z += c * B.z;
+        v1 += c * ldc<R, F>(a.b, j, c1);
+        v2 += c * ldc<R, F>(a.b, j, c2);
       }
     } else {
       for (int o = -C0; o <= C0; ++o) {
         const R c = a.tab->D[row][o + C0];
         if (c == (R)0) continue;
         const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
-        const V3<R> B = ld3(a.b + j);
-        v.x += c * B.x; v.y += c * B.y; v.z += c * B.z;
+        v1 += c * ldc<R, F>(a.b, j, c1);
+        v2 += c * ldc<R, F>(a.b, j, c2);
       }
     }
-    g[ax] = {v.x / a.dR[ax], v.y / a.dR[ax], v.z / a.dR[ax]};
+    g[ax][c1] = v1 * a.inv_d[ax];
+    g[ax][c2] = v2 * a.inv_d[ax];
   }
-  V3<R> c = {g[1].z - g[2].y, g[2].x - g[0].z, g[0].y - g[1].x};
+  V3<R> c = {g[1][2] - g[2][1], g[2][0] - g[0][2], g[0][1] - g[1][0]};
   if (a.rho) {
-    const R r = a.rho[idx];
-    c = {c.x / r, c.y / r, c.z / r};
+    const R r = (R)1 / a.rho[idx];
+    c = {c.x * r, c.y * r, c.z * r};
   }
-  st3(a.out + idx, c);
+  stf(a.out, idx, c);
 }
 
 // explicit launchers, instantiated per (R, OP) in stage_<r>_o<op>.cu
-template <typename R, int OP>
-void launch_stage(const StageArgs<R> &a, bool per, bool hall, int diss, dim3 grid, dim3 block,
+// conv: -1 decides per launch from StageArgs (conv / conv_flag); 0/1 fixes it at compile time
+template <typename R, typename F, int OP>
+void launch_stage(const StageArgs<R, F> &a, bool per, bool hall, int diss, int conv, dim3 grid, dim3 block,
                   cudaStream_t s);
-template <typename R, int OP>
-void launch_curl(const CurlArgs<R> &a, bool per, dim3 grid, dim3 block, cudaStream_t s);
+template <typename R, typename F, int OP>
+void launch_curl(const CurlArgs<R, F> &a, bool per, dim3 grid, dim3 block, cudaStream_t s);
+
+// layout conversion of a vector field between REAL4 AoS and SoA (fused path entry/exit)
+template <typename R>
+__global__ void k_aos_to_soa(long long n, const R4<R> *in, R *out, long long s) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3<R> v = ld3_plain(in + i);
+  out[i] = v.x;
+  out[i + s] = v.y;
+  out[i + 2 * s] = v.z;
+}
+template <typename R>
+__global__ void k_soa_to_aos(long long n, const R *in, long long s, R4<R> *out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  st3(out + i, V3<R>{in[i], in[i + s], in[i + 2 * s]});
+}
 
 }  // namespace ieq

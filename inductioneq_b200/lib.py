@@ -84,7 +84,8 @@ def load() -> ctypes.CDLL:
         getattr(lib, f).argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
     lib.ieq_compute_results.argtypes = [vp, vp, ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_double * 4)]
     lib.ieq_check_finite.argtypes = [vp, vp]
-    lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.POINTER(KernelRecord), ctypes.POINTER(ctypes.c_int)]
+    lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.POINTER(KernelRecord),
+                                                ctypes.POINTER(ctypes.c_int)]
     lib.ieq_status_string.argtypes = [ctypes.c_int]
     lib.ieq_status_string.restype = ctypes.c_char_p
     _LIB = lib
@@ -254,12 +255,13 @@ class Context:
                                                  ctypes.byref(out)))
         return {"abs_err": out[0], "rel_err": out[1], "divergence_norm": out[2], "energy": out[3]}
 
-    def profile_step(self, b, b2, b3, curlB_rho, u, rho, time) -> list[tuple[str, float]]:
-        """One step without a graph, with the device time of every kernel (ms)."""
+    def profile_step(self, b, b2, b3, curlB_rho, u, rho, time, repeats: int = 20) -> list[tuple[str, float]]:
+        """Average device time (ms) of every launch of one step, each timed alone in a graph of
+        `repeats` back-to-back launches; the fields hold no solution afterwards."""
         recs = (KernelRecord * 256)()
         n = ctypes.c_int(0)
         self._check(self.lib.ieq_profile_step(self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u),
-                                              _ptr(rho), _ptr(time), 256, recs, ctypes.byref(n)))
+                                              _ptr(rho), _ptr(time), int(repeats), 256, recs, ctypes.byref(n)))
         return [(recs[i].name.decode(), recs[i].ms) for i in range(min(n.value, 256))]
 
     def memset(self, buf, value: int = 0) -> None:
