@@ -157,6 +157,153 @@ def cpu_reference_run(steps: int, warmup: int, budget_s: float | None = None):
     return value, cores, kind, sample, el / done * NUM_STEPS_FULL
 
 
+# ------------------------------------------------------------------------------ other forms
+def events_time(stream, fn, reps=1):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / reps
+
+
+def form_fp32(dev, b_ref64):
+    """The same workload with REAL=float: DOF-updates/s and L2 error vs exact and vs FP64."""
+    import numpy as np
+    import torch
+    m = maps()
+    m.I_Tech["REAL"] = "float"
+    ctx = m.context(device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    b, b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho, t = ctx.scalar(), ctx.scalar(np.zeros(2), n=2)
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", u)
+    ctx.kernel("init_rho", rho)
+    b0 = ctx.get_vec(b)
+    flush = ctx.alloc(256 << 20)
+
+    def solve():
+        ctx.time_steps(b, b2, None, cb, u, rho, t, NUM_STEPS_FULL)
+
+    def reset():
+        b.upload(b0)
+        t.upload(np.zeros(2, dtype=np.float32))
+
+    reset()
+    solve()
+    reps, tt = 5, 0.0
+    for k in range(reps):
+        reset()
+        ctx.memset(flush, k)
+        tt += events_time(stream, solve)
+    res = ctx.results(b, T_FINAL, ctx.vec(), ctx.scalar())
+    b32 = ctx.get_vec(b).astype(np.float64)
+    vs64 = float(np.abs(b32 - b_ref64).max() / np.abs(b_ref64).max())
+    prof = ctx.profile_step(b, b2, None, cb, u, rho, t, repeats=20)
+    stage = statistics.mean([ms for nm, ms in prof if nm.startswith("stage")])
+    ctx.close()
+    value = 3 * N_GRID ** 3 * STAGES * NUM_STEPS_FULL * reps / tt
+    return {"value": value, "unit": "DOF/s", "ms_per_solve": tt / reps * 1e3, "l2_rel_err_vs_exact": res["rel_err"],
+            "max_rel_diff_vs_fp64": vs64, "stage_kernel_ms": stage,
+            "roofline": {"bound": "hbm", "achieved": 60 * N_GRID ** 3 / (stage * 1e-3) / 1e9, "unit": "GB/s",
+                         "algorithmic_bytes_per_node": 60},
+            "note": "same workload, FP32 state and stencils"}
+
+
+def form_batched(dev, steps=200):
+    """32 rotation solves, N ~ U{16..96}, omega ~ U(0.5,2), order in {2,4,6}, 200 SSPRK33 steps,
+    one persistent launch captured in a CUDA graph, tile shapes from the autotuner."""
+    import torch
+
+    from inductioneq_b200.batch import Batch, autotune, rotation_batch
+    specs = rotation_batch(32, seed=2026)
+    bt = Batch(specs, device=dev)
+    name = torch.cuda.get_device_name(dev)
+    tiles = autotune(bt, steps=3, gpu_name=name)
+    stream = torch.cuda.ExternalStream(bt.stream, device=dev)
+    flush = bt.ctxs[0].alloc(256 << 20)
+    out = {}
+    for persistent in (True, False):
+        bt.init()
+        bt.bind()
+        bt.run(steps, persistent=persistent)   # capture + warm
+        times = []
+        for k in range(3):
+            bt.bind()
+            bt.ctxs[0].memset(flush, k)
+            bt.ctxs[0].synchronize()
+            times.append(events_time(stream, lambda: bt.run(steps, persistent=persistent)))
+        tmin = statistics.median(times)
+        out["persistent" if persistent else "per_stage_launches"] = {
+            "value": 3 * bt.total_nodes * 3 * steps / tmin, "ms": tmin * 1e3}
+    bt.unbind()
+    err = []
+    for (n, o, om, dt), c, f in zip(specs, bt.ctxs, bt.fields):
+        res = c.results(f["b"], steps * dt, c.vec(), c.scalar())
+        err.append(res["rel_err"])
+    nodes = bt.total_nodes
+    grid = bt.grid()
+    bt.close()
+    best = out["persistent"]
+    t = best["ms"] * 1e-3
+    return {"value": best["value"], "unit": "DOF/s", "solves": len(specs), "total_nodes": nodes, "steps": steps,
+            "ms_per_run": best["ms"], "per_stage_launches_value": out["per_stage_launches"]["value"],
+            "persistent_grid": grid, "tiles": {k: list(v) for k, v in tiles.items()},
+            "l2_rel_err_vs_exact": {"min": min(err), "median": statistics.median(err), "max": max(err)},
+            "roofline": {"bound": "hbm", "achieved": 88 * nodes * 3 * steps / t / 1e9, "unit": "GB/s",
+                         "algorithmic_bytes_per_node_stage": 88},
+            "seed": 2026}
+
+
+def form_precision(dev, n=128, steps=20):
+    """Confined-domain Hall case on 128^3: FP32 state with FP64 CG cleaning to ||r||_2 < 1e-10,
+    then CK2N54 steps; compared with the FP64 run."""
+    import numpy as np
+    import torch
+
+    from inductioneq_b200.induction_eq import Maps
+    out = {}
+    fields = {}
+    for real in ("double", "float"):
+        m = Maps()
+        m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": 0.0, "XMAX": 1.0, "YMIN": 0.0,
+                         "YMAX": 1.0, "ZMIN": 0.0, "ZMAX": 1.0})
+        dx = 1.0 / (n - 1)
+        m.I_TI.update({"DT": 0.2 * dx * dx, "time_integrator": "CarpenterKennedy2N54"})
+        m.I_IEq.update({"hall_term": "USE_HALL"})
+        m.I_DC.update({"divergence_cleaning": True})
+        m.I_Tech["REAL"] = real
+        m.I_RunOps.update({"order": 4, "testcase": "confined_domain"})
+        ctx = m.context(device=dev)
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b).astype(np.float64)
+        bh[: ctx.n, :3] += 1e-3 * np.random.default_rng(12345).random((ctx.n, 3))
+        b.upload(bh.astype(ctx.real))
+        t0 = time.perf_counter()
+        cg = ctx.clean_div(b, 20000, 1e-10, check=False)
+        cg_s = time.perf_counter() - t0
+        b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec()
+        ctx.kernel("init_u", u)
+        rho, tt = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+        ctx.time_steps(b, b2, None, cb, u, rho, tt, 2)   # capture + warm
+        el = events_time(stream, lambda: ctx.time_steps(b, b2, None, cb, u, rho, tt, steps))
+        res = ctx.results(b, 0.0, ctx.vec(), ctx.scalar())
+        fields[real] = ctx.get_vec(b).astype(np.float64)
+        out[real] = {"dof_per_s": 3 * ctx.n * STAGES * steps / el, "cg_iterations": cg["iterations"],
+                     "cg_residual_norm2": cg["residual_norm2"], "cg_converged": cg["converged"],
+                     "cg_wall_s": cg_s, "divergence_norm_initial": cg["divergence_norm_initial"],
+                     "divergence_norm_after_steps": res["divergence_norm"]}
+        ctx.close()
+    diff = float(np.abs(fields["float"] - fields["double"]).max() / np.abs(fields["double"]).max())
+    return {"grid": [n] * 3, "steps": steps, "fp64": out["double"], "fp32_state_fp64_cg": out["float"],
+            "max_rel_diff_fp32_vs_fp64": diff}
+
+
 # ------------------------------------------------------------------------------ main
 def main() -> None:
     ap = argparse.ArgumentParser()
@@ -165,6 +312,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 / batched / precision lines")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -331,6 +479,21 @@ def main() -> None:
                      "divergence_norm": res["divergence_norm"]},
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not a.no_forms:
+        b_ref = None
+        try:
+            b.upload(b0)
+            tbuf.upload(np.zeros(2))
+            ctx.time_steps(b, b2, None, cb, u, rho, tbuf, NUM_STEPS_FULL)
+            b_ref = ctx.get_vec(b)
+            out["forms"] = {"fp32": form_fp32(dev, b_ref)}
+        except Exception as e:   # a form that fails is reported, not fatal to the line
+            out["forms"] = {"fp32": {"error": repr(e)}}
+        for name, fn in (("batched", form_batched), ("precision_c3", form_precision)):
+            try:
+                out["forms"][name] = fn(dev)
+            except Exception as e:
+                out["forms"][name] = {"error": repr(e)}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cv, cores, kind, sample, _ = cpu_reference_run(10 ** 6, 1, budget_s=15.0)
         out["cpu_baseline"] = {"value": cv, "unit": "DOF/s", "cores": cores, "kind": kind, "sample": sample}

@@ -150,6 +150,31 @@ ieq_status ieq_profile_step(ieq_ctx *ctx, void *b, void *b2, void *b3, void *cur
                             void *rho, void *time, int repeats, int max_records,
                             ieq_kernel_record *records, int *n_records);
 
+/* ---------------------------------------------------------------- batched form */
+
+/* Many independent solves of uneven grid sizes and SBP orders advanced together: every
+ * SSPRK33 stage of every solve is processed by one persistent kernel over a queue of tiles,
+ * the whole run captured in a CUDA graph.  No counterpart in the reference (which runs one
+ * grid per process); each solve is a context made by ieq_create, and the result of every
+ * solve equals ieq_time_steps on its own context.  Restrictions: REAL=double, SSPRK33,
+ * classical operators, no Hall term, no dissipation, constant velocity. */
+typedef struct ieq_batch ieq_batch;
+ieq_status ieq_batch_create(ieq_batch **batch, ieq_ctx *const *solves, int n_solves);
+void ieq_batch_destroy(ieq_batch *batch);
+const char *ieq_batch_last_error(const ieq_batch *batch);
+void *ieq_batch_stream(ieq_batch *batch);
+/* tile (brick) shape of one solve's tiles, tx*ty*tz = 256 nodes (chosen by the autotuner) */
+ieq_status ieq_batch_set_tile(ieq_batch *batch, int solve, int tx, int ty, int tz);
+/* fields[5*i + 0..4] = solve i's b, b2, b3, u, time (device pointers, reference layout) */
+ieq_status ieq_batch_bind(ieq_batch *batch, void *const *fields);
+/* num_steps steps of all bound solves; persistent = 0 launches one kernel per stage instead
+ * of one persistent kernel.  IEQ_ERR_TIMEOUT if a bounded grid barrier gave up.  Syncs. */
+ieq_status ieq_batch_run(ieq_batch *batch, int num_steps, int persistent);
+/* copy the solves' b, b2, b3 back into the bound fields */
+ieq_status ieq_batch_unbind(ieq_batch *batch);
+long long ieq_batch_total_tiles(const ieq_batch *batch);
+int ieq_batch_grid(const ieq_batch *batch);
+
 /* ---------------------------------------------------------------- allocation-free dot */
 
 /* FP64 dot product sum_i a[i]*b[i] of two device arrays of n doubles, written to the device

@@ -34,9 +34,34 @@ template <typename R>
 struct SoA {
   R *p;
   long long s;
+  int ro;     // (used by SoAcg only) the field is never written during the launch
+};
+// SoA read through L2 only (ld.global.cg), for a persistent kernel that reads, in a later
+// stage, data other blocks wrote in an earlier stage of the same launch; a field marked
+// `ro` (never written during the launch) keeps the read-only cached path
+template <typename R>
+struct SoAcg {
+  R *p;
+  long long s;
+  int ro;
 };
 template <typename R>
 __device__ __forceinline__ V3<R> ldf(const AoS<R> &f, long long j) { return ld3(f.p + j); }
+template <typename R>
+__device__ __forceinline__ V3<R> ldf(const SoAcg<R> &f, long long j) {
+  if (f.ro) return {__ldg(f.p + j), __ldg(f.p + j + f.s), __ldg(f.p + j + 2 * f.s)};
+  return {__ldcg(f.p + j), __ldcg(f.p + j + f.s), __ldcg(f.p + j + 2 * f.s)};
+}
+template <typename R>
+__device__ __forceinline__ V3<R> ldf_plain(const SoAcg<R> &f, long long j) {
+  return {__ldcg(f.p + j), __ldcg(f.p + j + f.s), __ldcg(f.p + j + 2 * f.s)};
+}
+template <typename R>
+__device__ __forceinline__ void stf(const SoAcg<R> &f, long long j, V3<R> v) {
+  f.p[j] = v.x;
+  f.p[j + f.s] = v.y;
+  f.p[j + 2 * f.s] = v.z;
+}
 template <typename R>
 __device__ __forceinline__ V3<R> ldf(const SoA<R> &f, long long j) {
   return {__ldg(f.p + j), __ldg(f.p + j + f.s), __ldg(f.p + j + 2 * f.s)};
@@ -224,18 +249,15 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R, F> &a, const int ii[3], co
   return acc;
 }
 
-template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV = -1>
-__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R, F> a) {
+// DB and the stage update at one node (ix, iy, iz) inside the grid.
+template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV>
+__device__ __forceinline__ void stage_node(const StageArgs<R, F> &a, int ix, int iy, int iz) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH;
   constexpr int RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
   constexpr bool HOD = DISS == DISS_HO;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const bool active = ix < nx && iy < ny && iz < nz;
-  if (active) {
+  {
     const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
     const int ii[3] = {ix, iy, iz};
     const int nn[3] = {nx, ny, nz};
@@ -387,6 +409,14 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
       }
     }
   }
+}
+
+template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV = -1>
+__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R, F> a) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix < a.m.nx && iy < a.m.ny && iz < a.m.nz) stage_node<R, F, OP, PER, HALL, DISS, CONV>(a, ix, iy, iz);
   // ---- time bookkeeping of the folded "a"/calc_time kernels, done by the last block
   if (a.tpost != TP_NONE) {
     __syncthreads();
