@@ -175,6 +175,30 @@ ieq_status ieq_batch_unbind(ieq_batch *batch);
 long long ieq_batch_total_tiles(const ieq_batch *batch);
 int ieq_batch_grid(const ieq_batch *batch);
 
+/* ---------------------------------------------------------------- discrete adjoint */
+
+/* Hand-written discrete adjoint of the spatial operator F(b) = DB (volume terms, Hall term
+ * with J = curl(b)/rho, high-order dissipation, inflow SAT) at fixed u and rho, and of the
+ * SSPRK33 step.  No counterpart in the reference.  FP64 only; Hall runs must be periodic (the
+ * Hall outflow SAT switches on the sign of 0.5u - J and has no adjoint); first-order and
+ * adaptive dissipation are not supported.  Vector fields in the reference layout. */
+/* out = F'(b) v (tangent linear) */
+ieq_status ieq_operator_jvp(ieq_ctx *ctx, const void *b, const void *v, const void *u, const void *rho,
+                            void *out);
+/* out = F'(b)^T w */
+ieq_status ieq_operator_vjp(ieq_ctx *ctx, const void *b, const void *w, const void *u, const void *rho,
+                            void *out);
+/* lambda <- (d b_{n+1} / d b_n)^T lambda for one SSPRK33 step with stage states s1 = b_n,
+ * s2 = b^(2), s3 = b^(3) starting at time t0 (u from u_analytical at the stage times when
+ * -DIEQ_VARIABLE_U=1, else the given u) */
+ieq_status ieq_ssprk33_step_vjp(ieq_ctx *ctx, const void *s1, const void *s2, const void *s3, double t0,
+                                void *lambda, const void *u, const void *rho);
+/* Gradient through num_steps SSPRK33 steps from b0 at t = 0: lambda holds dL/db(T) on entry
+ * and dL/db0 on return.  The forward run is checkpointed every checkpoint_every steps and
+ * each segment recomputed (stage states kept) during the reverse sweep. */
+ieq_status ieq_adjoint_steps(ieq_ctx *ctx, const void *b0, void *lambda, const void *u, const void *rho,
+                             int num_steps, int checkpoint_every);
+
 /* ---------------------------------------------------------------- allocation-free dot */
 
 /* FP64 dot product sum_i a[i]*b[i] of two device arrays of n doubles, written to the device

@@ -1,0 +1,531 @@
+// adjoint.cu -- discrete adjoint of the semi-discretisation and of SSPRK33.
+//
+// F(b) is the time derivative DB of kernel/kernel_time_integrator.cl:9-31 (volume terms,
+// Hall term with J = curl(b)/rho, artificial dissipation, inflow SAT) at fixed u and rho.
+// Three operators are provided, all FP64:
+//   jvp:  F'(b0) v    (tangent linear; used by the transpose tests)
+//   vjp:  F'(b0)^T w  (the adjoint of the spatial operator)
+//   SSPRK33 step adjoint: lambda_n = (d b_{n+1} / d b_n)^T lambda_{n+1} from the stage states
+// The transposes are written out per term (see the notes at k_vjp_pass1); D^T is applied as
+// a gather over the neighbours j = k + p with the coefficient of row(j) at offset -p.
+// The Hall outflow SAT (a switch on the sign of 0.5u - J) has no adjoint here: Hall runs
+// must be periodic.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ieq_host.h"
+
+#include "stage_kernel.cuh"
+
+namespace ieq {
+
+struct AdjArgs {
+  Mesh m;
+  const Tables<double> *tab;
+  int nb, sw, wh, periodic;
+  int conv, hall, hod;
+  double hod_factor;
+  double w[6];           // flux-form weights (see stage_kernel.cuh)
+  double inv_d[3], two_inv_d[3], sat_s[3];
+  const R4<double> *b0, *J0, *u, *v, *dJ;   // v: tangent direction or adjoint input w
+  const double *rho;
+  R4<double> *out;
+  R4<double> *gJr;       // vjp pass 1 -> pass 2: (Hall adjoint source for J) / rho
+};
+
+__device__ __forceinline__ V3<double> ld(const R4<double> *p, long long j) { return ld3(p + j); }
+__device__ __forceinline__ double comp(V3<double> v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+__device__ __forceinline__ void addc(V3<double> &v, int c, double x) {
+  if (c == 0) v.x += x;
+  else if (c == 1) v.y += x;
+  else v.z += x;
+}
+__device__ __forceinline__ V3<double> axpy3(double a, V3<double> x, V3<double> y) {
+  return {a * x.x + y.x, a * x.y + y.y, a * x.z + y.z};
+}
+__device__ __forceinline__ double dot3(V3<double> a, V3<double> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct Node {
+  int i[3], n[3];
+  long long st[3], idx;
+};
+
+__device__ __forceinline__ int row_of(const AdjArgs &a, int i, int n) {
+  return a.periodic ? a.nb : sbp_row(i, n, a.nb);
+}
+
+// neighbour j = node + o along axis; false if outside a non-periodic grid
+__device__ __forceinline__ bool nbr_idx(const AdjArgs &a, const Node &nd, int ax, int o, long long &j, int &jj) {
+  int t = nd.i[ax] + o;
+  if (a.periodic) {
+    t += (t < 0) ? nd.n[ax] : 0;
+    t -= (t >= nd.n[ax]) ? nd.n[ax] : 0;
+  } else if (t < 0 || t >= nd.n[ax]) {
+    return false;
+  }
+  jj = t;
+  j = nd.idx + (long long)(t - nd.i[ax]) * nd.st[ax];
+  return true;
+}
+
+// forward derivative row at the node: sum_o D[row][o] f(node + o)
+template <typename Fn>
+__device__ V3<double> dfwd(const AdjArgs &a, const Node &nd, int ax, Fn f) {
+  const int c0 = (a.sw - 1) / 2;
+  const int r = row_of(a, nd.i[ax], nd.n[ax]);
+  V3<double> s = {0, 0, 0};
+  for (int o = -c0; o <= c0; ++o) {
+    const double c = a.tab->D[r][o + c0];
+    if (c == 0.0) continue;
+    long long j;
+    int jj;
+    if (!nbr_idx(a, nd, ax, o, j, jj)) continue;
+    s = axpy3(c, f(j), s);
+  }
+  return s;
+}
+
+// transposed derivative at the node: sum_j D[row(j)][node - j] f(j)
+template <typename Fn>
+__device__ V3<double> dtr(const AdjArgs &a, const Node &nd, int ax, Fn f) {
+  const int c0 = (a.sw - 1) / 2;
+  V3<double> s = {0, 0, 0};
+  for (int p = -c0; p <= c0; ++p) {
+    long long j;
+    int jj;
+    if (!nbr_idx(a, nd, ax, p, j, jj)) continue;
+    const double c = a.tab->D[row_of(a, jj, nd.n[ax])][c0 - p];
+    if (c == 0.0) continue;
+    s = axpy3(c, f(j), s);
+  }
+  return s;
+}
+
+// dissipation row (symmetric use: forward with the row of the node, transpose with rows of j)
+template <bool TR>
+__device__ V3<double> hod_apply(const AdjArgs &a, const Node &nd, int ax, const R4<double> *x) {
+  const int h0 = a.wh - 1;
+  V3<double> s = {0, 0, 0};
+  for (int p = -h0; p <= h0; ++p) {
+    long long j;
+    int jj;
+    if (!nbr_idx(a, nd, ax, p, j, jj)) continue;
+    const double c = TR ? a.tab->H[row_of(a, jj, nd.n[ax])][h0 - p] : a.tab->H[row_of(a, nd.i[ax], nd.n[ax])][h0 + p];
+    if (c == 0.0) continue;
+    s = axpy3(c, ld(x, j), s);
+  }
+  return s;
+}
+
+__device__ __forceinline__ bool make_node(const AdjArgs &a, Node &nd) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= a.m.nx || iy >= a.m.ny || iz >= a.m.nz) return false;
+  nd.i[0] = ix; nd.i[1] = iy; nd.i[2] = iz;
+  nd.n[0] = a.m.nx; nd.n[1] = a.m.ny; nd.n[2] = a.m.nz;
+  nd.st[0] = 1; nd.st[1] = a.m.nx; nd.st[2] = (long long)a.m.nx * a.m.ny;
+  nd.idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+  return true;
+}
+
+// SAT of the inflow boundary (induction_Eq_surface.cl:7-33): linear in b with the diagonal
+// coefficient sum_a s_a c_a u_a on the faces
+__device__ double sat_diag(const AdjArgs &a, const Node &nd, V3<double> um) {
+  if (a.periodic || a.hall || !a.conv) return 0.0;
+  double d = 0.0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const bool l = nd.i[ax] == 0, r = nd.i[ax] == nd.n[ax] - 1;
+    const double ua = comp(um, ax);
+    const double c = (l && ua > 0 ? -1.0 : 0.0) + (r && ua < 0 ? 1.0 : 0.0);
+    d += (a.sat_s[ax] * c) * ua;
+  }
+  return d;
+}
+
+// tangent linear F'(b0) v; dJ = curl(v)/rho precomputed
+__global__ void k_jvp(const AdjArgs a) {
+  Node nd;
+  if (!make_node(a, nd)) return;
+  const long long k = nd.idx;
+  const V3<double> vm = ld(a.v, k), um = a.conv ? ld(a.u, k) : V3<double>{0, 0, 0};
+  V3<double> out = {0, 0, 0};
+  for (int ax = 0; ax < 3; ++ax) {
+    if (a.conv) {
+      // the factored split forms with b -> v (linear in b at fixed u)
+      const V3<double> DuiBa = dfwd(a, nd, ax, [&](long long j) {
+        const V3<double> uu = ld(a.u, j);
+        const double va = comp(ld(a.v, j), ax);
+        return V3<double>{uu.x * va, uu.y * va, uu.z * va};
+      });
+      const V3<double> DU = dfwd(a, nd, ax, [&](long long j) { return ld(a.u, j); });
+      const V3<double> DV = dfwd(a, nd, ax, [&](long long j) { return ld(a.v, j); });
+      const V3<double> DuaB = dfwd(a, nd, ax, [&](long long j) {
+        const V3<double> vv = ld(a.v, j);
+        const double ua = comp(ld(a.u, j), ax);
+        return V3<double>{ua * vv.x, ua * vv.y, ua * vv.z};
+      });
+      const double va = comp(vm, ax), ua = comp(um, ax), DVa = comp(DV, ax), DUa = comp(DU, ax);
+      for (int i = 0; i < 3; ++i) {
+        const double vol = a.w[0] * comp(DuiBa, i) + a.w[1] * va * comp(DU, i) + a.w[2] * comp(um, i) * DVa -
+                           (a.w[3] * comp(DuaB, i) + a.w[4] * ua * comp(DV, i) + a.w[5] * comp(vm, i) * DUa);
+        addc(out, i, a.two_inv_d[ax] * vol);
+      }
+    }
+    if (a.hall) {
+      // D_a[dJ_a b0 + J0_a v - dJ b0_a - J0 v_a]
+      const V3<double> s = dfwd(a, nd, ax, [&](long long j) {
+        const V3<double> b = ld(a.b0, j), J = ld(a.J0, j), v = ld(a.v, j), dJ = ld(a.dJ, j);
+        const double dJa = comp(dJ, ax), Ja = comp(J, ax), ba = comp(b, ax), va = comp(v, ax);
+        return V3<double>{dJa * b.x + Ja * v.x - dJ.x * ba - J.x * va, dJa * b.y + Ja * v.y - dJ.y * ba - J.y * va,
+                          dJa * b.z + Ja * v.z - dJ.z * ba - J.z * va};
+      });
+      out = axpy3(a.inv_d[ax], s, out);
+    }
+    if (a.hod) out = axpy3(a.hod_factor, hod_apply<false>(a, nd, ax, a.v), out);
+  }
+  out = axpy3(sat_diag(a, nd, um), vm, out);
+  st3(a.out + k, out);
+}
+
+// F'(b0)^T w, pass 1.  With q_a = D_a^T w (per component), the forward terms transpose to
+//   D_a[u_i b_a]      -> z_a += sum_i u_i q_a,i          b_a D_a[u_i] -> z_a += D_a[u] . w
+//   u_i D_a[b_a]      -> z_a += D_a^T[u . w]             D_a[u_a b_i] -> z_i += u_a q_a,i
+//   u_a D_a[b_i]      -> z_i += D_a^T[u_a w_i]           b_i D_a[u_a] -> z_i += D_a[u_a] w_i
+// (times the flux-form weights and 2/d_a); the Hall term with Q_a = q_a / d_a gives
+//   z_i += J0_a Q_a,i,  z_a -= J0 . Q_a,  and the source for dJ: gJ = sum_a (b0.Q_a) e_a - b0_a Q_a,
+// whose curl transpose (pass 2) adds C^T (gJ / rho).
+__global__ void k_vjp_pass1(const AdjArgs a) {
+  Node nd;
+  if (!make_node(a, nd)) return;
+  const long long k = nd.idx;
+  const V3<double> wm = ld(a.v, k), um = a.conv ? ld(a.u, k) : V3<double>{0, 0, 0};
+  V3<double> z = {0, 0, 0}, gJ = {0, 0, 0};
+  V3<double> b0m = {0, 0, 0}, J0m = {0, 0, 0};
+  if (a.hall) {
+    b0m = ld(a.b0, k);
+    J0m = ld(a.J0, k);
+  }
+  for (int ax = 0; ax < 3; ++ax) {
+    const V3<double> q = dtr(a, nd, ax, [&](long long j) { return ld(a.v, j); });
+    if (a.conv) {
+      const V3<double> Du = dfwd(a, nd, ax, [&](long long j) { return ld(a.u, j); });
+      const V3<double> S3 = dtr(a, nd, ax, [&](long long j) {
+        const double s = dot3(ld(a.u, j), ld(a.v, j));
+        return V3<double>{s, 0, 0};
+      });
+      const V3<double> S5 = dtr(a, nd, ax, [&](long long j) {
+        const double ua = comp(ld(a.u, j), ax);
+        const V3<double> ww = ld(a.v, j);
+        return V3<double>{ua * ww.x, ua * ww.y, ua * ww.z};
+      });
+      const double ua = comp(um, ax), Dua = comp(Du, ax);
+      addc(z, ax, a.two_inv_d[ax] * (a.w[0] * dot3(um, q) + a.w[1] * dot3(Du, wm) + a.w[2] * S3.x));
+      for (int i = 0; i < 3; ++i)
+        addc(z, i, -a.two_inv_d[ax] * (a.w[3] * ua * comp(q, i) + a.w[4] * comp(S5, i) + a.w[5] * Dua * comp(wm, i)));
+    }
+    if (a.hall) {
+      const V3<double> Q = {q.x * a.inv_d[ax], q.y * a.inv_d[ax], q.z * a.inv_d[ax]};
+      const double J0a = comp(J0m, ax), b0a = comp(b0m, ax);
+      z = axpy3(J0a, Q, z);
+      addc(z, ax, -dot3(J0m, Q));
+      addc(gJ, ax, dot3(b0m, Q));
+      gJ = axpy3(-b0a, Q, gJ);
+    }
+    if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+  }
+  z = axpy3(sat_diag(a, nd, um), wm, z);
+  st3(a.out + k, z);
+  if (a.hall) {
+    const double r = 1.0 / a.rho[k];
+    st3(a.gJr + k, V3<double>{gJ.x * r, gJ.y * r, gJ.z * r});
+  }
+}
+
+// pass 2: z += C^T g with C the SBP curl (rows / d), g = gJ / rho
+__global__ void k_vjp_pass2(const AdjArgs a) {
+  Node nd;
+  if (!make_node(a, nd)) return;
+  const long long k = nd.idx;
+  V3<double> g[3];
+  for (int ax = 0; ax < 3; ++ax) {
+    const V3<double> t = dtr(a, nd, ax, [&](long long j) { return ld(a.gJr, j); });
+    g[ax] = {t.x * a.inv_d[ax], t.y * a.inv_d[ax], t.z * a.inv_d[ax]};   // (D_ax^T g_c) / d_ax
+  }
+  // (C^T g)_x = Dz^T g_y - Dy^T g_z, (C^T g)_y = Dx^T g_z - Dz^T g_x, (C^T g)_z = Dy^T g_x - Dx^T g_y
+  V3<double> z = ld3_plain(a.out + k);
+  z.x += g[2].y - g[1].z;
+  z.y += g[0].z - g[2].x;
+  z.z += g[1].x - g[0].y;
+  st3(a.out + k, z);
+}
+
+// out = alpha*x + beta*y (+ gamma*z) over the nodes (x, y, z may be the same array as out)
+__global__ void k_lincomb(long long n, R4<double> *out, double al, const R4<double> *x, double be,
+                          const R4<double> *y, double ga, const R4<double> *z) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  V3<double> r = {0, 0, 0};
+  if (x) r = axpy3(al, ld3_plain(x + i), r);
+  if (y) r = axpy3(be, ld3_plain(y + i), r);
+  if (z) r = axpy3(ga, ld3_plain(z + i), r);
+  st3(out + i, r);
+}
+
+}  // namespace ieq
+
+using namespace ieq;
+
+namespace ieq {
+// from api.cu
+ieq_status adj_run_kernel(ieq_ctx *c, const char *name, void *const *args, int nargs);
+void adj_curl(ieq_ctx *c, const void *b, const void *rho, void *out);
+void adj_context(ieq_ctx *c, Mesh &m, const Tables<double> *&tab, double w[6], double inv_d[3], double two_inv_d[3],
+                 double sat_s[3]);
+
+AdjArgs adj_args(ieq_ctx *c) {
+  AdjArgs a;
+  std::memset(&a, 0, sizeof(a));
+  adj_context(c, a.m, a.tab, a.w, a.inv_d, a.two_inv_d, a.sat_s);
+  a.nb = c->op.nb;
+  a.sw = c->op.sw;
+  a.wh = c->op.w_hod;
+  a.periodic = c->s.periodic ? 1 : 0;
+  a.conv = 1;
+  a.hall = c->s.hall ? 1 : 0;
+  a.hod = c->s.diss_form == 1 ? 1 : 0;
+  a.hod_factor = c->s.hod_factor;
+  return a;
+}
+}  // namespace ieq
+
+namespace {
+
+ieq_status afail(ieq_ctx *c, ieq_status st, const std::string &m) {
+  c->err = m;
+  return st;
+}
+
+ieq_status check_adjoint_settings(ieq_ctx *c) {
+  if (c->s.real_float) return afail(c, IEQ_ERR_SETTINGS, "the adjoint is FP64 only");
+  if (c->s.hall && !c->s.periodic) return afail(c, IEQ_ERR_SETTINGS, "the Hall outflow SAT has no adjoint: Hall runs must be periodic");
+  if (c->s.diss_form == 2 || c->s.diss_form == 3)
+    return afail(c, IEQ_ERR_SETTINGS, "first-order/adaptive dissipation has no adjoint");
+  if (c->s.uibj < 0 || c->s.source < 0 || c->s.ujbi < 0) return afail(c, IEQ_ERR_SETTINGS, "no flux forms");
+  return IEQ_OK;
+}
+
+dim3 ablock() { return dim3(32, 4, 2); }
+dim3 agrid(const ieq_ctx *c) {
+  return dim3((c->s.nodes[0] + 31) / 32, (c->s.nodes[1] + 3) / 4, (c->s.nodes[2] + 1) / 2);
+}
+
+struct Work {
+  void *J0 = nullptr, *dJ = nullptr, *gJr = nullptr;
+};
+
+ieq_status work_alloc(ieq_ctx *c, std::vector<void *> &bufs, int n, size_t bytes) {
+  for (int i = 0; i < n; ++i) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return afail(c, IEQ_ERR_CUDA, "adjoint work allocation");
+    cudaMemsetAsync(p, 0, bytes, c->stream);
+    bufs.push_back(p);
+  }
+  return IEQ_OK;
+}
+
+void free_all(std::vector<void *> &bufs) {
+  for (void *p : bufs) cudaFree(p);
+  bufs.clear();
+}
+
+// out = F'(b)^T w (u at the stage time, rho); J0, gJr: work fields
+ieq_status vjp(ieq_ctx *c, const void *b, const void *w, const void *u, const void *rho, void *out, void *J0,
+               void *gJr) {
+  AdjArgs a = adj_args(c);
+  a.b0 = (const R4<double> *)b;
+  a.u = (const R4<double> *)u;
+  a.v = (const R4<double> *)w;
+  a.rho = (const double *)rho;
+  a.out = (R4<double> *)out;
+  a.gJr = (R4<double> *)gJr;
+  if (c->s.hall) {
+    adj_curl(c, b, rho, J0);
+    a.J0 = (const R4<double> *)J0;
+  }
+  k_vjp_pass1<<<agrid(c), ablock(), 0, c->stream>>>(a);
+  if (c->s.hall) k_vjp_pass2<<<agrid(c), ablock(), 0, c->stream>>>(a);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? IEQ_OK : afail(c, IEQ_ERR_CUDA, cudaGetErrorString(e));
+}
+
+void lincomb(ieq_ctx *c, void *out, double al, const void *x, double be, const void *y, double ga = 0,
+             const void *z = nullptr) {
+  const long long n = (long long)c->n;
+  k_lincomb<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, (R4<double> *)out, al, (const R4<double> *)x, be,
+                                                               (const R4<double> *)y, ga, (const R4<double> *)z);
+}
+
+// u at stage time t (calc_u with time[1] = t) into `uw`, or the caller's u
+const void *stage_u(ieq_ctx *c, const void *u, void *uw, double *d_time, double t) {
+  if (!c->s.variable_u) return u;
+  double tt[2] = {t, t};
+  cudaMemcpyAsync(d_time, tt, sizeof(tt), cudaMemcpyHostToDevice, c->stream);
+  void *args[7] = {uw, uw, uw, uw, uw, uw, d_time};   // calc_u_3_args reads u (4) and time (6)
+  adj_run_kernel(c, "calc_u_3_args", args, 7);
+  return uw;
+}
+
+}  // namespace
+
+extern "C" {
+
+ieq_status ieq_operator_jvp(ieq_ctx *c, const void *b, const void *v, const void *u, const void *rho, void *out) {
+  if (!c || !b || !v || !u || !rho || !out) return IEQ_ERR_ARG;
+  ieq_status st = check_adjoint_settings(c);
+  if (st != IEQ_OK) return st;
+  cudaSetDevice(c->device);
+  std::vector<void *> w;
+  if ((st = work_alloc(c, w, 2, c->n_pad * sizeof(R4<double>))) != IEQ_OK) return st;
+  AdjArgs a = adj_args(c);
+  a.b0 = (const R4<double> *)b;
+  a.u = (const R4<double> *)u;
+  a.v = (const R4<double> *)v;
+  a.rho = (const double *)rho;
+  a.out = (R4<double> *)out;
+  if (c->s.hall) {
+    adj_curl(c, b, rho, w[0]);
+    adj_curl(c, v, rho, w[1]);
+    a.J0 = (const R4<double> *)w[0];
+    a.dJ = (const R4<double> *)w[1];
+  }
+  k_jvp<<<agrid(c), ablock(), 0, c->stream>>>(a);
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  free_all(w);
+  return e == cudaSuccess ? IEQ_OK : afail(c, IEQ_ERR_CUDA, cudaGetErrorString(e));
+}
+
+ieq_status ieq_operator_vjp(ieq_ctx *c, const void *b, const void *w, const void *u, const void *rho, void *out) {
+  if (!c || !b || !w || !u || !rho || !out) return IEQ_ERR_ARG;
+  ieq_status st = check_adjoint_settings(c);
+  if (st != IEQ_OK) return st;
+  cudaSetDevice(c->device);
+  std::vector<void *> bufs;
+  if ((st = work_alloc(c, bufs, 2, c->n_pad * sizeof(R4<double>))) != IEQ_OK) return st;
+  st = vjp(c, b, w, u, rho, out, bufs[0], bufs[1]);
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  free_all(bufs);
+  if (st != IEQ_OK) return st;
+  return e == cudaSuccess ? IEQ_OK : afail(c, IEQ_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// Adjoint of one SSPRK33 step (kernel_time_integrator.cl:224-303) from its stage states
+// s1 = b_n, s2 = b^(2), s3 = b^(3) and the step start time t0: lambda <- (db_{n+1}/db_n)^T lambda.
+//   b2 = s1 + h F(s1, t0)            b3 = 3/4 s1 + 1/4 (s2 + h F(s2, t0 + h))
+//   b_{n+1} = 1/3 s1 + 2/3 (s3 + h F(s3, t0 + h/2))
+ieq_status ieq_ssprk33_step_vjp(ieq_ctx *c, const void *s1, const void *s2, const void *s3, double t0, void *lambda,
+                                const void *u, const void *rho) {
+  if (!c || !s1 || !s2 || !s3 || !lambda || !u || !rho) return IEQ_ERR_ARG;
+  ieq_status st = check_adjoint_settings(c);
+  if (st != IEQ_OK) return st;
+  cudaSetDevice(c->device);
+  std::vector<void *> w;
+  const size_t vb = c->n_pad * sizeof(R4<double>);
+  if ((st = work_alloc(c, w, 7, vb)) != IEQ_OK) return st;
+  void *J0 = w[0], *gJr = w[1], *z = w[2], *l1 = w[3], *l2 = w[4], *l3 = w[5], *uw = w[6];
+  double *d_time = nullptr;
+  cudaMalloc(&d_time, 2 * sizeof(double));
+  const double h = c->s.dt;
+  const double t2 = t0 + h, t3 = t0 + 0.5 * h;   // SSPRK33_2a / _3a
+  // stage 3: lambda3 = 2/3 (lambda + h F'(s3)^T lambda); lambda1 = 1/3 lambda
+  if ((st = vjp(c, s3, lambda, stage_u(c, u, uw, d_time, t3), rho, z, J0, gJr)) != IEQ_OK) goto done;
+  lincomb(c, l3, 2.0 / 3.0, lambda, 2.0 / 3.0 * h, z);
+  lincomb(c, l1, 1.0 / 3.0, lambda, 0.0, nullptr);
+  // stage 2: lambda2 = 1/4 (lambda3 + h F'(s2)^T lambda3); lambda1 += 3/4 lambda3
+  if ((st = vjp(c, s2, l3, stage_u(c, u, uw, d_time, t2), rho, z, J0, gJr)) != IEQ_OK) goto done;
+  lincomb(c, l2, 0.25, l3, 0.25 * h, z);
+  lincomb(c, l1, 1.0, l1, 0.75, l3);
+  // stage 1: lambda1 += lambda2 + h F'(s1)^T lambda2
+  if ((st = vjp(c, s1, l2, stage_u(c, u, uw, d_time, t0), rho, z, J0, gJr)) != IEQ_OK) goto done;
+  lincomb(c, lambda, 1.0, l1, 1.0, l2, h, z);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = afail(c, IEQ_ERR_CUDA, "step vjp");
+done:
+  cudaStreamSynchronize(c->stream);
+  cudaFree(d_time);
+  free_all(w);
+  return st;
+}
+
+// Adjoint of num_steps SSPRK33 steps from b0 (time 0): lambda holds dL/db(T) on entry and
+// dL/db0 on return.  The forward run is checkpointed every `checkpoint_every` steps; each
+// segment is recomputed (stage states kept) and swept backwards.
+ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const void *u, const void *rho, int num_steps,
+                             int checkpoint_every) {
+  if (!c || !b0 || !lambda || !u || !rho || num_steps < 0 || checkpoint_every < 1) return IEQ_ERR_ARG;
+  ieq_status st = check_adjoint_settings(c);
+  if (st != IEQ_OK) return st;
+  if (c->s.integrator != "SSPRK33") return afail(c, IEQ_ERR_SETTINGS, "the adjoint time stepping is SSPRK33");
+  cudaSetDevice(c->device);
+  const size_t vb = c->n_pad * sizeof(R4<double>);
+  const int K = checkpoint_every;
+  const int nseg = (num_steps + K - 1) / K;
+  std::vector<void *> ck, seg, w;
+  if ((st = work_alloc(c, ck, nseg, vb)) != IEQ_OK || (st = work_alloc(c, seg, 3 * K, vb)) != IEQ_OK ||
+      (st = work_alloc(c, w, 5, vb)) != IEQ_OK) {
+    free_all(ck);
+    free_all(seg);
+    free_all(w);
+    return st;
+  }
+  void *cur = w[0], *b2 = w[1], *b3 = w[2], *cb = w[3], *uw = w[4];
+  double *d_time = nullptr;
+  cudaMalloc(&d_time, 2 * sizeof(double));
+  std::vector<double> t0s(num_steps + 1, 0.0);
+  for (int n = 0; n < num_steps; ++n) t0s[n + 1] = t0s[n] + c->s.dt;   // calc_time_3_args
+  auto step = [&](void *state, double t0, void *keep1, void *keep2, void *keep3) -> ieq_status {
+    // one SSPRK33 step through the reference kernels, keeping the stage states
+    double tt[2] = {t0, t0};
+    cudaMemcpyAsync(d_time, tt, sizeof(tt), cudaMemcpyHostToDevice, c->stream);
+    if (keep1) cudaMemcpyAsync(keep1, state, vb, cudaMemcpyDeviceToDevice, c->stream);
+    void *ua = c->s.variable_u ? uw : (void *)u;
+    void *args[7] = {state, b2, b3, cb, ua, (void *)rho, d_time};
+    const char *seq[] = {"calc_curlB_rho_1_3args", "calc_u_3_args", "SSPRK33_1", "SSPRK33_2a",
+                         "calc_curlB_rho_2_3args", "calc_u_3_args", "SSPRK33_2b", "SSPRK33_3a",
+                         "calc_curlB_rho_3_3args", "calc_u_3_args", "SSPRK33_3b"};
+    for (const char *k : seq) {
+      if (!c->s.hall && std::strncmp(k, "calc_curlB", 10) == 0) continue;
+      if (!c->s.variable_u && std::strncmp(k, "calc_u", 6) == 0) continue;
+      ieq_status s = adj_run_kernel(c, k, args, 7);
+      if (s != IEQ_OK) return s;
+      if (std::strcmp(k, "SSPRK33_1") == 0 && keep2) cudaMemcpyAsync(keep2, b2, vb, cudaMemcpyDeviceToDevice, c->stream);
+      if (std::strcmp(k, "SSPRK33_2b") == 0 && keep3) cudaMemcpyAsync(keep3, b3, vb, cudaMemcpyDeviceToDevice, c->stream);
+    }
+    return IEQ_OK;
+  };
+  // forward sweep with checkpoints
+  cudaMemcpyAsync(cur, b0, vb, cudaMemcpyDeviceToDevice, c->stream);
+  for (int n = 0; n < num_steps && st == IEQ_OK; ++n) {
+    if (n % K == 0) cudaMemcpyAsync(ck[n / K], cur, vb, cudaMemcpyDeviceToDevice, c->stream);
+    st = step(cur, t0s[n], nullptr, nullptr, nullptr);
+  }
+  // reverse sweep
+  for (int s = nseg - 1; s >= 0 && st == IEQ_OK; --s) {
+    const int n0 = s * K, n1 = std::min(num_steps, n0 + K);
+    cudaMemcpyAsync(cur, ck[s], vb, cudaMemcpyDeviceToDevice, c->stream);
+    for (int n = n0; n < n1 && st == IEQ_OK; ++n)
+      st = step(cur, t0s[n], seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2]);
+    for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n)
+      st = ieq_ssprk33_step_vjp(c, seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2], t0s[n], lambda, u,
+                                rho);
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "adjoint sweep");
+  cudaFree(d_time);
+  free_all(ck);
+  free_all(seg);
+  free_all(w);
+  return st;
+}
+
+}  // extern "C"

@@ -585,6 +585,25 @@ ieq_status run_one_any(ieq_ctx *c, const char *name, const uint32_t *g, void *co
 
 }  // namespace
 
+// ---- helpers of the adjoint (adjoint.cu)
+#include "adjoint_args.inc"
+
+namespace ieq {
+// pieces of a context that adjoint.cu needs to build its kernel arguments
+void adj_context(ieq_ctx *c, Mesh &m, const Tables<double> *&tab, double w[6], double inv_d[3], double two_inv_d[3],
+                 double sat_s[3]) {
+  m = mesh_of(c);
+  tab = tables<double>(c);
+  const Forms f = flux_forms(c->s);
+  for (int k = 0; k < 6; ++k) w[k] = f.w[k];
+  for (int a = 0; a < 3; ++a) {
+    inv_d[a] = 1.0 / c->s.d[a];
+    two_inv_d[a] = 2.0 / c->s.d[a];
+    sat_s[a] = c->op.minv[0] / c->s.d[a];
+  }
+}
+}  // namespace ieq
+
 // default NDRange of every reference kernel (used by the typed entry points)
 static ieq_status ieq_run_one_default(ieq_ctx *ctx, const char *name, void *const *args, int nargs) {
   if (!ctx) return IEQ_ERR_ARG;

@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(256) k_cg_update(Mesh m, int off, int gx, int 
 }
 
 // initial residual r = div B: rr = <r, r> from reduction partials, and the loop condition
-__global__ void k_cg_start(const double *partials_rr, int np, CgState *cs, double *history) {
+static __global__ void k_cg_start(const double *partials_rr, int np, CgState *cs, double *history) {
   const double rr = block_sum_partials(partials_rr, np);
   if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
     cs->rr = rr;

@@ -36,9 +36,11 @@ struct SoA {
   long long s;
   int ro;     // (used by SoAcg only) the field is never written during the launch
 };
-// SoA read through L2 only (ld.global.cg), for a persistent kernel that reads, in a later
-// stage, data other blocks wrote in an earlier stage of the same launch; a field marked
-// `ro` (never written during the launch) keeps the read-only cached path
+// SoA for a persistent kernel that reads, in a later stage, data other blocks wrote in an
+// earlier stage of the same launch.  Such data must not go through the non-coherent
+// read-only path (ld.global.nc); ordinary loads (ld.global.ca) issued after the fenced grid
+// barrier observe the other blocks' writes.  A field marked `ro` (never written during the
+// launch) keeps the read-only path.
 template <typename R>
 struct SoAcg {
   R *p;
@@ -50,11 +52,11 @@ __device__ __forceinline__ V3<R> ldf(const AoS<R> &f, long long j) { return ld3(
 template <typename R>
 __device__ __forceinline__ V3<R> ldf(const SoAcg<R> &f, long long j) {
   if (f.ro) return {__ldg(f.p + j), __ldg(f.p + j + f.s), __ldg(f.p + j + 2 * f.s)};
-  return {__ldcg(f.p + j), __ldcg(f.p + j + f.s), __ldcg(f.p + j + 2 * f.s)};
+  return {__ldca(f.p + j), __ldca(f.p + j + f.s), __ldca(f.p + j + 2 * f.s)};
 }
 template <typename R>
 __device__ __forceinline__ V3<R> ldf_plain(const SoAcg<R> &f, long long j) {
-  return {__ldcg(f.p + j), __ldcg(f.p + j + f.s), __ldcg(f.p + j + 2 * f.s)};
+  return {__ldca(f.p + j), __ldca(f.p + j + f.s), __ldca(f.p + j + 2 * f.s)};
 }
 template <typename R>
 __device__ __forceinline__ void stf(const SoAcg<R> &f, long long j, V3<R> v) {

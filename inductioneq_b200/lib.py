@@ -86,6 +86,10 @@ def load() -> ctypes.CDLL:
     lib.ieq_check_finite.argtypes = [vp, vp]
     lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.POINTER(KernelRecord),
                                                 ctypes.POINTER(ctypes.c_int)]
+    lib.ieq_operator_jvp.argtypes = [vp] * 6
+    lib.ieq_operator_vjp.argtypes = [vp] * 6
+    lib.ieq_ssprk33_step_vjp.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, vp, vp]
+    lib.ieq_adjoint_steps.argtypes = [vp] * 5 + [ctypes.c_int, ctypes.c_int]
     lib.ieq_status_string.argtypes = [ctypes.c_int]
     lib.ieq_status_string.restype = ctypes.c_char_p
     _LIB = lib
@@ -263,6 +267,21 @@ class Context:
         self._check(self.lib.ieq_profile_step(self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u),
                                               _ptr(rho), _ptr(time), int(repeats), 256, recs, ctypes.byref(n)))
         return [(recs[i].name.decode(), recs[i].ms) for i in range(min(n.value, 256))]
+
+    # ---------------------------------------------------------------- discrete adjoint
+    def operator_jvp(self, b, v, u, rho, out) -> None:
+        self._check(self.lib.ieq_operator_jvp(self.h, _ptr(b), _ptr(v), _ptr(u), _ptr(rho), _ptr(out)))
+
+    def operator_vjp(self, b, w, u, rho, out) -> None:
+        self._check(self.lib.ieq_operator_vjp(self.h, _ptr(b), _ptr(w), _ptr(u), _ptr(rho), _ptr(out)))
+
+    def ssprk33_step_vjp(self, s1, s2, s3, t0: float, lam, u, rho) -> None:
+        self._check(self.lib.ieq_ssprk33_step_vjp(self.h, _ptr(s1), _ptr(s2), _ptr(s3), float(t0), _ptr(lam),
+                                                  _ptr(u), _ptr(rho)))
+
+    def adjoint_steps(self, b0, lam, u, rho, num_steps: int, checkpoint_every: int = 10) -> None:
+        self._check(self.lib.ieq_adjoint_steps(self.h, _ptr(b0), _ptr(lam), _ptr(u), _ptr(rho), int(num_steps),
+                                               int(checkpoint_every)))
 
     def memset(self, buf, value: int = 0) -> None:
         self._check(self.lib.ieq_memset(self.h, _ptr(buf), value, buf.nbytes))

@@ -1,0 +1,176 @@
+"""Discrete adjoint on the GPU.
+
+* transpose tests: <w, F'(b) v> = <F'(b)^T w, v> for the tangent-linear and adjoint spatial
+  operators of several configurations (relative 1e-12);
+* the tangent against central differences of the forward operator;
+* the checkpointed SSPRK33 gradient of a final-time L2 misfit against central differences
+  along seeded random directions (relative 1e-6), driven through a torch.autograd.Function
+  (defined here, in the test harness only).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from tests.helpers import maps_for
+
+pytestmark = pytest.mark.gpu
+
+HP = 4.0 * math.pi / 3.0
+CASES = {
+    "hallper_4c": dict(order=4, testcase="hall_periodic", nodes=(16, 17, 18), lo=0.0, hi=HP, periodic=True, hall=True,
+                       integrator="SSPRK33", variable_u=True),
+    "hallper_6c_hod": dict(order=6, testcase="hall_periodic", nodes=(16, 16, 16), lo=0.0, hi=HP, periodic=True,
+                           hall=True, dissipation="HIGH_ORDER", integrator="SSPRK33"),
+    "rot_6c_sat": dict(order=6, testcase="rotation_gaussian", nodes=(14, 15, 16), lo=-1.0, hi=1.0,
+                       integrator="SSPRK33"),
+    "rot3d_4e_split_hod": dict(order=4, extended=True, testcase="rotation_3D", nodes=(14, 13, 15), lo=-1.0, hi=1.0,
+                               uibj="SPLIT", source="SPLIT", ujbi="PRODUCT", dissipation="HIGH_ORDER",
+                               integrator="SSPRK33"),
+}
+
+
+def _setup(c, dt=1.0):
+    ctx = maps_for(dict(c, dt=dt)).context()
+    b, u = ctx.vec(), ctx.vec()
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", u)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    return ctx, b, u, rho
+
+
+def _rand(ctx, seed):
+    r = np.random.default_rng(seed).standard_normal((ctx.n_pad, 4))
+    r[:, 3] = 0
+    r[ctx.n:] = 0
+    return r
+
+
+def _dot(a, b):
+    return float(np.sum(a[:, :3] * b[:, :3]))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_operator_transpose(name):
+    ctx, b, u, rho = _setup(CASES[name])
+    v, w = _rand(ctx, 1), _rand(ctx, 2)
+    dv, dw, jv, jtw = ctx.vec(v), ctx.vec(w), ctx.vec(), ctx.vec()
+    ctx.operator_jvp(b, dv, u, rho, jv)
+    ctx.operator_vjp(b, dw, u, rho, jtw)
+    lhs = _dot(w, ctx.get_vec(jv))
+    rhs = _dot(ctx.get_vec(jtw), v)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def _F(ctx, b, u, rho, hall):
+    """DB(b) through the reference kernels (CarpenterKennedy2N54_1a: b2 = DT*DB(b1), DT = 1)."""
+    b2, cb, t = ctx.vec(), ctx.vec(), ctx.scalar(np.zeros(2), n=2)
+    names = (["calc_curlB_rho_1_2args"] if hall else []) + ["CarpenterKennedy2N54_1a"]
+    ctx.run(names, ctx_nodes(ctx), b, b2, cb, u, rho, t)
+    return ctx.get_vec(b2)
+
+
+def ctx_nodes(ctx):
+    return ctx._nodes
+
+
+@pytest.mark.parametrize("name", ["hallper_4c", "rot_6c_sat"])
+def test_tangent_matches_central_differences(name):
+    c = dict(CASES[name], integrator="CarpenterKennedy2N54")
+    ctx, b, u, rho = _setup(c)
+    ctx._nodes = c["nodes"]
+    b0 = ctx.get_vec(b)
+    v = _rand(ctx, 3) * 1e-2
+    jv = ctx.vec()
+    ctx.operator_jvp(b, ctx.vec(v), u, rho, jv)
+    eps = 1e-4
+    fp = _F(ctx, ctx.vec(b0 + eps * v), u, rho, c.get("hall", False))
+    fm = _F(ctx, ctx.vec(b0 - eps * v), u, rho, c.get("hall", False))
+    fd = (fp - fm) / (2 * eps)
+    got = ctx.get_vec(jv)
+    assert np.abs(fd - got)[:, :3].max() <= 1e-6 * np.abs(got[:, :3]).max()
+
+
+def _c5_small():
+    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16))
+    ctx = maps_for(dict(c, dt=1.0)).context()
+    u = ctx.vec()
+    ctx.kernel("init_u", u)
+    umax = float(np.sqrt((ctx.get_vec(u)[:, :3] ** 2).sum(1)).max())
+    dx = HP / 16
+    dt = (2.0 / 16) * dx / umax        # CFL 2/N (compute_error_hall_periodic.m:51)
+    ctx.close()
+    return maps_for(dict(c, dt=dt)).context(), dt
+
+
+def test_checkpointed_gradient_matches_central_differences_via_autograd():
+    torch = pytest.importorskip("torch")
+    ctx, dt = _c5_small()
+    nsteps, every = 12, 5
+    b = ctx.vec()
+    ctx.kernel("init_b", b)
+    u = ctx.vec()
+    ctx.kernel("init_u", u)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    b0 = ctx.get_vec(b)
+    n = ctx.n
+
+    def forward_np(x):
+        bb, b2, b3, cb = ctx.vec(x), ctx.vec(), ctx.vec(), ctx.vec()
+        uu = ctx.vec()
+        ctx.kernel("init_u", uu)
+        t = ctx.scalar(np.zeros(2), n=2)
+        ctx.time_steps(bb, b2, b3, cb, uu, rho, t, nsteps)
+        return ctx.get_vec(bb)
+
+    class Evolve(torch.autograd.Function):
+        """B(T) = Phi(B0) with the adjoint sweep as backward (test harness only)."""
+
+        @staticmethod
+        def forward(fctx, x):
+            fctx.save_for_backward(x)
+            return torch.from_numpy(forward_np(x.detach().cpu().numpy()))
+
+        @staticmethod
+        def backward(fctx, g):
+            (x,) = fctx.saved_tensors
+            lam = ctx.vec(g.detach().cpu().numpy())
+            uu = ctx.vec()
+            ctx.kernel("init_u", uu)
+            ctx.adjoint_steps(ctx.vec(x.detach().cpu().numpy()), lam, uu, rho, nsteps, every)
+            return torch.from_numpy(ctx.get_vec(lam))
+
+    # mass weights of ||.||_M (kernel_operator.cl:22-28): periodic -> dx dy dz
+    wmass = (HP / 16) ** 3
+    rng = np.random.default_rng(2026)
+    target = forward_np(b0) + 1e-3 * rng.standard_normal((ctx.n_pad, 4))
+    target[:, 3] = 0
+    target[n:] = 0
+    tt = torch.from_numpy(target)
+
+    def loss(x):
+        d = Evolve.apply(x) - tt
+        return 0.5 * wmass * (d[:, :3] ** 2).sum()
+
+    x = torch.from_numpy(b0.copy()).requires_grad_(True)
+    L = loss(x)
+    L.backward()
+    g = x.grad.numpy()
+    def fd(d, eps):
+        with torch.no_grad():
+            Lp = float(loss(torch.from_numpy(b0 + eps * d)))
+            Lm = float(loss(torch.from_numpy(b0 - eps * d)))
+        return (Lp - Lm) / (2 * eps)
+
+    for k in range(6):
+        d = rng.standard_normal((ctx.n_pad, 4))
+        d[:, 3] = 0
+        d[n:] = 0
+        d /= np.sqrt(np.sum(d[:, :3] ** 2))          # unit l2 direction
+        ad = float(np.sum(g[:, :3] * d[:, :3]))
+        # central differences converge as eps^2 onto the adjoint directional derivative
+        e1, e2 = abs(fd(d, 1e-3) - ad), abs(fd(d, 1e-4) - ad)
+        assert e2 <= 1e-6 * abs(ad), (k, e1, e2, ad)
+        assert e2 <= 0.05 * e1 or e2 <= 1e-9 * abs(ad), (k, e1, e2)
