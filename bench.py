@@ -304,6 +304,88 @@ def form_precision(dev, n=128, steps=20):
             "max_rel_diff_fp32_vs_fp64": diff}
 
 
+def form_adjoint(dev, n=64, t_final=0.2, every=10, n_dirs=20):
+    """Hall periodic (include/hall_periodic.h) 64^3, FP64, 4th order, variable u, SSPRK33 at CFL 2/N
+    to t = 0.2: gradient of J = 1/2 ||B(T) - B_tgt||_M^2 (B_tgt = exact(T) + seeded N(0, 1e-3)) with
+    respect to B0 by the checkpointed adjoint, checked against Richardson-extrapolated central
+    differences along seeded unit directions."""
+    import numpy as np
+
+    from inductioneq_b200.induction_eq import Maps
+    hp = 4.0 * math.pi / 3.0
+
+    def mk(dt):
+        m = Maps()
+        m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": 0.0, "XMAX": hp, "YMIN": 0.0, "YMAX": hp,
+                         "ZMIN": 0.0, "ZMAX": hp})
+        m.I_TI.update({"DT": dt, "time_integrator": "SSPRK33"})
+        m.I_IEq.update({"hall_term": "USE_HALL"})
+        m.I_RunOps.update({"order": 4, "testcase": "hall_periodic", "periodic": "USE_PERIODIC", "variable_u": True})
+        return m.context(device=dev)
+
+    ctx = mk(1.0)
+    u = ctx.vec()
+    ctx.kernel("init_u", u)
+    umax = float(np.sqrt((ctx.get_vec(u)[:, :3] ** 2).sum(1)).max())
+    ctx.close()
+    dx = hp / n
+    dt = (2.0 / n) * dx / umax                      # initialize.m:93-99 with CFL 2/N
+    steps = math.ceil(t_final / dt)
+    dt = t_final / steps
+    ctx = mk(dt)
+    b, b2, b3, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    ctx.kernel("init_b", b)
+    b0 = ctx.get_vec(b)
+    wmass = dx ** 3
+    tb = ctx.scalar(np.array([t_final, t_final]), n=2)
+    ana = ctx.vec()
+    ctx.run("analytical_b", (n, n, n), ana, tb)
+    rng = np.random.default_rng(2026)
+    target = ctx.get_vec(ana)
+    target[: ctx.n, :3] += 1e-3 * rng.standard_normal((ctx.n, 3))
+
+    def forward(x):
+        b.upload(x)
+        ctx.kernel("init_u", u)
+        t = ctx.scalar(np.zeros(2), n=2)
+        ctx.time_steps(b, b2, b3, cb, u, rho, t, steps)
+        return ctx.get_vec(b)
+
+    def loss(x):
+        d = forward(x)[: ctx.n, :3] - target[: ctx.n, :3]
+        return 0.5 * wmass * float(np.sum(d * d))
+
+    t0 = time.perf_counter()
+    bT = forward(b0)
+    t_fwd = time.perf_counter() - t0
+    lam = ctx.vec()
+    g = np.zeros_like(bT)
+    g[: ctx.n, :3] = wmass * (bT[: ctx.n, :3] - target[: ctx.n, :3])
+    lam.upload(g)
+    t0 = time.perf_counter()
+    ctx.adjoint_steps(ctx.vec(b0), lam, u, rho, steps, every)
+    t_adj = time.perf_counter() - t0
+    grad = ctx.get_vec(lam)
+    worst = 0.0
+    for k in range(n_dirs):
+        d = rng.standard_normal(b0.shape)
+        d[:, 3] = 0
+        d[ctx.n:] = 0
+        d /= np.sqrt(np.sum(d[:, :3] ** 2))
+        ad = float(np.sum(grad[:, :3] * d[:, :3]))
+        eps = 1e-3
+
+        def cd(e):
+            return (loss(b0 + e * d) - loss(b0 - e * d)) / (2 * e)
+        fd = (4.0 * cd(eps / 2) - cd(eps)) / 3.0          # Richardson: O(eps^4)
+        worst = max(worst, abs(fd - ad) / abs(ad))
+    ctx.close()
+    return {"grid": [n] * 3, "steps": steps, "dt": dt, "checkpoint_every": every, "forward_s": t_fwd,
+            "adjoint_s": t_adj, "fd_directions": n_dirs, "fd": "Richardson-extrapolated central differences, eps 1e-3 and 5e-4",
+            "max_rel_diff_vs_fd": worst}
+
+
 # ------------------------------------------------------------------------------ main
 def main() -> None:
     ap = argparse.ArgumentParser()
@@ -489,7 +571,7 @@ def main() -> None:
             out["forms"] = {"fp32": form_fp32(dev, b_ref)}
         except Exception as e:   # a form that fails is reported, not fatal to the line
             out["forms"] = {"fp32": {"error": repr(e)}}
-        for name, fn in (("batched", form_batched), ("precision_c3", form_precision)):
+        for name, fn in (("batched", form_batched), ("precision_c3", form_precision), ("adjoint_c5", form_adjoint)):
             try:
                 out["forms"][name] = fn(dev)
             except Exception as e:
