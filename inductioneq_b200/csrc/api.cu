@@ -8,7 +8,7 @@
 
 #include "ieq_host.h"
 #include "misc_kernels.cuh"
-#include "stage_kernel.cuh"
+#include "stage_col.cuh"
 
 using namespace ieq;
 
@@ -213,8 +213,40 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
   }
 }
 
+template <typename R>
+void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv) {
+  const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
+  switch (c->op_id) {
+    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, c->stream); break;
+    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, c->stream); break;
+    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, c->stream); break;
+    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, c->stream); break;
+    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, c->stream); break;
+    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, c->stream); break;
+  }
+}
+
 template <typename R, typename F>
-void launch_curl_any(ieq_ctx *c, F b, const R *rho, F out) {
+CurlArgs<R, F> curl_args(ieq_ctx *c, F b, const R *rho, F out);
+
+// E = J x B with J = curl(b)/rho, and J on the faces of a non-periodic box
+template <typename R>
+void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jface) {
+  CurlArgs<R, SoA<R>> a = curl_args<R, SoA<R>>(c, b, rho, E);
+  a.jface = jface;
+  const bool per = c->s.periodic;
+  switch (c->op_id) {
+    case 0: launch_curl_e<R, 0>(a, per, c->stream); break;
+    case 1: launch_curl_e<R, 1>(a, per, c->stream); break;
+    case 2: launch_curl_e<R, 2>(a, per, c->stream); break;
+    case 3: launch_curl_e<R, 3>(a, per, c->stream); break;
+    case 4: launch_curl_e<R, 4>(a, per, c->stream); break;
+    case 5: launch_curl_e<R, 5>(a, per, c->stream); break;
+  }
+}
+
+template <typename R, typename F>
+CurlArgs<R, F> curl_args(ieq_ctx *c, F b, const R *rho, F out) {
   CurlArgs<R, F> a;
   std::memset(&a, 0, sizeof(a));
   a.m = mesh_of(c);
@@ -229,6 +261,12 @@ void launch_curl_any(ieq_ctx *c, F b, const R *rho, F out) {
     a.dR[ax] = (R)c->s.d[ax];
     a.inv_d[ax] = (R)(1.0 / c->s.d[ax]);
   }
+  return a;
+}
+
+template <typename R, typename F>
+void launch_curl_any(ieq_ctx *c, F b, const R *rho, F out) {
+  const CurlArgs<R, F> a = curl_args<R, F>(c, b, rho, out);
   const dim3 g = grid3(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2]), bl = block3();
   const bool per = c->s.periodic;
   switch (c->op_id) {

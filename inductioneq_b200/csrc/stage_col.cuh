@@ -1,0 +1,399 @@
+// stage_col.cuh -- the column form of the fused stage kernel and of curl(B)/rho, used by
+// the time stepping on the structure-of-arrays state.
+//
+// Each thread advances a column of NZ nodes adjacent in z (IEQ_COL_NODES).  The x and y
+// derivative rows are gathered per node as in k_stage; along z the nodes of a column share
+// their stencil planes: the planes iz0-RI .. iz0+NZ-1+RI are loaded once and each is
+// accumulated into every node's sums with its own coefficient.  A column that meets the
+// SBP boundary rows in z (non-periodic box) falls back to per-node gathers.
+//
+// Hall term.  The Hall volume flux of axis a at a stencil point k is J_a B_i - J_i B_a
+// (induction_Eq_volume.cl Hall_volume), an entry of the antisymmetric tensor of J and B
+// whose three independent entries are E = (Jx By - Jy Bx, Jx Bz - Jz Bx, Jy Bz - Jz By).
+// k_curl_e computes J = curl(B)/rho and writes E (and J itself on the faces of a
+// non-periodic box, where the outflow SAT needs it), so the stage kernel reads two values
+// per stencil point and axis instead of six and forms no products there.
+#pragma once
+#include "stage_kernel.cuh"
+
+namespace ieq {
+
+// Nodes per thread along z and the register cap (via resident blocks of 128 threads).
+// Measured on B200 for the 6th-order Hall + HOD stage (64^3 .. 128^3): one node per thread
+// at <= 64 registers (8 blocks per SM) beats two- and four-node columns, whose extra
+// registers cost more latency hiding than the shared z planes save.
+#ifndef IEQ_COL_NODES
+#define IEQ_COL_NODES 1
+#endif
+#ifndef IEQ_COL_MIN_BLOCKS
+#define IEQ_COL_MIN_BLOCKS 8
+#endif
+#ifndef IEQ_CURL_NODES
+#define IEQ_CURL_NODES 1
+#endif
+constexpr int kColNodes = IEQ_COL_NODES;     // nodes per thread along z (stage kernel)
+constexpr int kCurlNodes = IEQ_CURL_NODES;   // nodes per thread along z (curl kernel)
+// the convection terms keep twelve sums per node and axis: one node per thread there
+__host__ __device__ constexpr int col_nodes(int conv) { return conv ? 1 : kColNodes; }
+
+template <typename R>
+__device__ __forceinline__ R cmp(const V3<R> &v, int ax) {
+  return ax == 0 ? v.x : (ax == 1 ? v.y : v.z);
+}
+
+template <typename R>
+struct ColSums {
+  V3<R> SuiBa, SU, SB, SuaB, SHo;
+  R h1, h2;   // sum_k c_k E_c1(k), sum_k c_k E_c2(k) (see e_comp*)
+};
+
+// The two entries of E the Hall flux of axis ax needs, and their signs in DB:
+//   ax 0: DB_y += D[Exy], DB_z += D[Exz];  ax 1: DB_x -= D[Exy], DB_z += D[Eyz];
+//   ax 2: DB_x -= D[Exz], DB_y -= D[Eyz]
+__host__ __device__ constexpr int e_comp1(int ax) { return ax == 2 ? 1 : 0; }
+__host__ __device__ constexpr int e_comp2(int ax) { return ax == 0 ? 1 : 2; }
+
+// one stencil point: dterm adds the derivative-row terms (conv, Hall), hterm the dissipation
+template <typename R, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_acc(ColSums<R> &s, int ax, int need, R cD, R cH, bool dterm, bool hterm,
+                                        const V3<R> &B, const V3<R> &U, R e1, R e2) {
+  if (CONV && dterm) {
+    const R Ba = cmp(B, ax), Ua = cmp(U, ax);
+    if (need & 1) {
+      s.SuiBa.x += cD * (U.x * Ba); s.SuiBa.y += cD * (U.y * Ba); s.SuiBa.z += cD * (U.z * Ba);
+    }
+    if (need & 2) { s.SU.x += cD * U.x; s.SU.y += cD * U.y; s.SU.z += cD * U.z; }
+    if (need & 4) { s.SB.x += cD * B.x; s.SB.y += cD * B.y; s.SB.z += cD * B.z; }
+    if (need & 8) {
+      s.SuaB.x += cD * (Ua * B.x); s.SuaB.y += cD * (Ua * B.y); s.SuaB.z += cD * (Ua * B.z);
+    }
+  }
+  if (HALL && dterm) {
+    s.h1 += cD * e1;
+    s.h2 += cD * e2;
+  }
+  if (HOD && hterm) {
+    s.SHo.x += cH * B.x; s.SHo.y += cH * B.y; s.SHo.z += cH * B.z;
+  }
+}
+
+template <typename R, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_load(const StageArgs<R, SoA<R>> &a, int ax, long long j, V3<R> &B, V3<R> &U,
+                                         R &e1, R &e2) {
+  if (CONV || HOD) B = ldf(a.bk, j);
+  if (CONV) U = ldf(a.u, j);
+  if (HALL) {
+    e1 = __ldg(a.E.p + j + e_comp1(ax) * a.E.s);
+    e2 = __ldg(a.E.p + j + e_comp2(ax) * a.E.s);
+  }
+}
+
+// the sums of one axis at one node (interior row, periodic wrap or SBP boundary row)
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, SoA<R>> &a, int ax, int i, int n,
+                                         long long idx, long long st, const V3<R> &Bm) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
+  constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
+  const V3<R> zero = {0, 0, 0};
+  const int row = PER ? NB : sbp_row(i, n, NB);
+  if (row == NB) {
+    const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+    for (int o = -RI; o <= RI; ++o) {
+      if (o == 0) {
+        // the interior derivative rows have a zero centre
+        if (HOD) col_acc<R, false, HOD, 0>(s, ax, 0, (R)0, a.Hint[RI], false, true, Bm, zero, (R)0, (R)0);
+        continue;
+      }
+      const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st : idx + (long long)o * st;
+      V3<R> B = zero, U = zero;
+      R e1 = 0, e2 = 0;
+      col_load<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
+      col_acc<R, HALL, HOD, CONV>(s, ax, a.need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
+    }
+  } else {
+    for (int o = -RB; o <= RB; ++o) {
+      const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+      const R cH = (HOD && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+      if (cD == (R)0 && cH == (R)0) continue;
+      const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st;
+      V3<R> B = zero, U = zero;
+      R e1 = 0, e2 = 0;
+      col_load<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
+      col_acc<R, HALL, HOD, CONV>(s, ax, a.need, cD, cH, cD != (R)0, cH != (R)0, B, U, e1, e2);
+    }
+  }
+}
+
+// add one axis' sums into DB (volume and Hall terms) and the dissipation sum
+template <typename R, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_combine(const StageArgs<R, SoA<R>> &a, int ax, const ColSums<R> &s,
+                                            const V3<R> &Bm, const V3<R> &um, V3<R> &db, V3<R> &hod) {
+  if (CONV) {
+    const R Ba = cmp(Bm, ax), Ua = cmp(um, ax);
+    const R SBa = cmp(s.SB, ax), SUa = cmp(s.SU, ax);
+    const R *w = a.w;
+    V3<R> vol;
+    vol.x = w[0] * s.SuiBa.x + w[1] * Ba * s.SU.x + w[2] * um.x * SBa -
+            (w[3] * s.SuaB.x + w[4] * Ua * s.SB.x + w[5] * Bm.x * SUa);
+    vol.y = w[0] * s.SuiBa.y + w[1] * Ba * s.SU.y + w[2] * um.y * SBa -
+            (w[3] * s.SuaB.y + w[4] * Ua * s.SB.y + w[5] * Bm.y * SUa);
+    vol.z = w[0] * s.SuiBa.z + w[1] * Ba * s.SU.z + w[2] * um.z * SBa -
+            (w[3] * s.SuaB.z + w[4] * Ua * s.SB.z + w[5] * Bm.z * SUa);
+    db.x += a.two_inv_d[ax] * vol.x;
+    db.y += a.two_inv_d[ax] * vol.y;
+    db.z += a.two_inv_d[ax] * vol.z;
+  }
+  if (HALL) {
+    const R f1 = a.inv_d[ax] * s.h1, f2 = a.inv_d[ax] * s.h2;
+    if (ax == 0) {
+      db.y += f1; db.z += f2;
+    } else if (ax == 1) {
+      db.x -= f1; db.z += f2;
+    } else {
+      db.x -= f1; db.y -= f2;
+    }
+  }
+  if (HOD) {
+    hod.x += s.SHo.x; hod.y += s.SHo.y; hod.z += s.SHo.z;
+  }
+}
+
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+__global__ void __launch_bounds__(128, CONV ? 2 : IEQ_COL_MIN_BLOCKS) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+  constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
+  constexpr int NZ = col_nodes(CONV);
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz0 = (blockIdx.z * blockDim.z + threadIdx.z) * NZ;
+  if (ix < nx && iy < ny && iz0 < nz) {
+    const int cnt = nz - iz0 < NZ ? nz - iz0 : NZ;
+    const long long sz = (long long)nx * ny;
+    const long long base = ix + (long long)nx * iy;
+    const V3<R> zero = {0, 0, 0};
+    V3<R> Bm[NZ], um[NZ], db[NZ], hod[NZ];
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      db[k] = zero;
+      hod[k] = zero;
+      Bm[k] = zero;
+      um[k] = zero;
+      if (k < cnt) {
+        const long long idx = base + (long long)(iz0 + k) * sz;
+        Bm[k] = ldf(a.bk, idx);
+        if (CONV) um[k] = ldf(a.u, idx);
+      }
+    }
+    // x and y: per-node gathers
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      if (k < cnt) {
+        const long long idx = base + (long long)(iz0 + k) * sz;
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+          ColSums<R> s{};
+          col_axis<R, OP, PER, HALL, HOD, CONV>(s, a, ax, ax == 0 ? ix : iy, ax == 0 ? nx : ny, idx,
+                                                ax == 0 ? 1 : nx, Bm[k]);
+          col_combine<R, HALL, HOD, CONV>(a, ax, s, Bm[k], um[k], db[k], hod[k]);
+        }
+      }
+    }
+    // z: shared stencil planes when the whole column uses the interior row
+    const bool stream = cnt == NZ && (PER || (sbp_row(iz0, nz, NB) == NB && sbp_row(iz0 + NZ - 1, nz, NB) == NB));
+    if (stream) {
+      ColSums<R> s[NZ];
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) s[k] = ColSums<R>{};
+#pragma unroll
+      for (int p = -RI; p <= NZ - 1 + RI; ++p) {
+        int zz = iz0 + p;
+        if (PER) {
+          zz += zz < 0 ? nz : 0;
+          zz -= zz >= nz ? nz : 0;
+        }
+        const long long j = base + (long long)zz * sz;
+        V3<R> B = zero, U = zero;
+        R e1 = 0, e2 = 0;
+        if (p >= 0 && p < NZ) {
+          B = Bm[p];
+          U = um[p];
+          if (HALL) {
+            e1 = __ldg(a.E.p + j + e_comp1(2) * a.E.s);
+            e2 = __ldg(a.E.p + j + e_comp2(2) * a.E.s);
+          }
+        } else {
+          col_load<R, HALL, HOD, CONV>(a, 2, j, B, U, e1, e2);
+        }
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+          const int o = p - k;
+          if (o < -RI || o > RI) continue;
+          if (o == 0) {
+            if (HOD) col_acc<R, false, HOD, 0>(s[k], 2, 0, (R)0, a.Hint[RI], false, true, B, zero, (R)0, (R)0);
+          } else {
+            col_acc<R, HALL, HOD, CONV>(s[k], 2, a.need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) col_combine<R, HALL, HOD, CONV>(a, 2, s[k], Bm[k], um[k], db[k], hod[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) {
+        if (k < cnt) {
+          const long long idx = base + (long long)(iz0 + k) * sz;
+          ColSums<R> s{};
+          col_axis<R, OP, PER, HALL, HOD, CONV>(s, a, 2, iz0 + k, nz, idx, sz, Bm[k]);
+          col_combine<R, HALL, HOD, CONV>(a, 2, s, Bm[k], um[k], db[k], hod[k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      if (k < cnt) {
+        const int ii[3] = {ix, iy, iz0 + k};
+        const int nn[3] = {nx, ny, nz};
+        const long long idx = base + (long long)(iz0 + k) * sz;
+        V3<R> d = db[k];
+        if (!PER) stage_sat<R, SoA<R>, HALL>(a, ii, nn, idx, Bm[k], um[k], CONV, d);
+        if (HOD) {
+          d.x += a.hod_factor * hod[k].x;
+          d.y += a.hod_factor * hod[k].y;
+          d.z += a.hod_factor * hod[k].z;
+        }
+        stage_epilogue<R, SoA<R>>(a, idx, d);
+      }
+    }
+  }
+  stage_time_post(a);
+}
+
+// J = curl(B)/rho and E = J x B, two nodes per thread along z (see the file comment)
+template <typename R, int OP, bool PER>
+__global__ void __launch_bounds__(128) k_curl_e(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
+  constexpr int NZ = kCurlNodes;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz0 = (blockIdx.z * blockDim.z + threadIdx.z) * NZ;
+  if (ix >= nx || iy >= ny || iz0 >= nz) return;
+  const int cnt = nz - iz0 < NZ ? nz - iz0 : NZ;
+  const long long sz = (long long)nx * ny;
+  const long long base = ix + (long long)nx * iy;
+  const int nn[3] = {nx, ny, nz};
+  const long long st[3] = {1, nx, sz};
+  R g[NZ][3][3];   // g[node][axis][component]
+  // one axis at one node: the derivatives of the two components orthogonal to it
+  auto axis = [&](int ax, int i, long long idx, R &v1, R &v2) {
+    const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+    v1 = 0;
+    v2 = 0;
+    const int row = PER ? NB : sbp_row(i, nn[ax], NB);
+    if (row == NB) {
+      const bool wrap = PER && (i < RI || i >= nn[ax] - RI);
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) {
+        if (o == 0) continue;
+        const R c = a.Dint[o + RI];
+        const long long j = wrap ? idx + (long long)(nbr<true>(i, o, nn[ax]) - i) * st[ax] : idx + (long long)o * st[ax];
+        v1 += c * __ldg(a.b.p + j + c1 * a.b.s);
+        v2 += c * __ldg(a.b.p + j + c2 * a.b.s);
+      }
+    } else {
+      for (int o = -C0; o <= C0; ++o) {
+        const R c = a.tab->D[row][o + C0];
+        if (c == (R)0) continue;
+        const long long j = idx + (long long)(nbr<PER>(i, o, nn[ax]) - i) * st[ax];
+        v1 += c * __ldg(a.b.p + j + c1 * a.b.s);
+        v2 += c * __ldg(a.b.p + j + c2 * a.b.s);
+      }
+    }
+  };
+#pragma unroll
+  for (int k = 0; k < NZ; ++k) {
+    if (k < cnt) {
+      const long long idx = base + (long long)(iz0 + k) * sz;
+#pragma unroll
+      for (int ax = 0; ax < 2; ++ax) {
+        R v1, v2;
+        axis(ax, ax == 0 ? ix : iy, idx, v1, v2);
+        g[k][ax][(ax + 1) % 3] = v1 * a.inv_d[ax];
+        g[k][ax][(ax + 2) % 3] = v2 * a.inv_d[ax];
+      }
+    }
+  }
+  const bool stream = cnt == NZ && (PER || (sbp_row(iz0, nz, NB) == NB && sbp_row(iz0 + NZ - 1, nz, NB) == NB));
+  if (stream) {
+    R v1[NZ], v2[NZ];
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) v1[k] = v2[k] = 0;
+#pragma unroll
+    for (int p = -RI; p <= NZ - 1 + RI; ++p) {
+      // the plane is used by some node at a non-zero offset
+      bool used = false;
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) used |= (p - k >= -RI && p - k <= RI && p != k);
+      if (!used) continue;
+      int zz = iz0 + p;
+      if (PER) {
+        zz += zz < 0 ? nz : 0;
+        zz -= zz >= nz ? nz : 0;
+      }
+      const long long j = base + (long long)zz * sz;
+      const R bx = __ldg(a.b.p + j), by = __ldg(a.b.p + j + a.b.s);
+#pragma unroll
+      for (int k = 0; k < NZ; ++k) {
+        const int o = p - k;
+        if (o < -RI || o > RI || o == 0) continue;
+        v1[k] += a.Dint[o + RI] * bx;
+        v2[k] += a.Dint[o + RI] * by;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      g[k][2][0] = v1[k] * a.inv_d[2];
+      g[k][2][1] = v2[k] * a.inv_d[2];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      if (k < cnt) {
+        R v1, v2;
+        axis(2, iz0 + k, base + (long long)(iz0 + k) * sz, v1, v2);
+        g[k][2][0] = v1 * a.inv_d[2];
+        g[k][2][1] = v2 * a.inv_d[2];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NZ; ++k) {
+    if (k < cnt) {
+      const int iz = iz0 + k;
+      const long long idx = base + (long long)iz * sz;
+      V3<R> J = {g[k][1][2] - g[k][2][1], g[k][2][0] - g[k][0][2], g[k][0][1] - g[k][1][0]};
+      if (a.rho) {
+        const R r = (R)1 / a.rho[idx];
+        J = {J.x * r, J.y * r, J.z * r};
+      }
+      const V3<R> B = ldf(a.b, idx);
+      stf(a.out, idx, V3<R>{J.x * B.y - J.y * B.x, J.x * B.z - J.z * B.x, J.y * B.z - J.z * B.y});
+      if (!PER && (ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1))
+        stf(a.jface, idx, J);
+    }
+  }
+}
+
+// launch shape of the column kernels: 32 x 4 threads, each `nodes` nodes in z
+inline dim3 col_block() { return dim3(32, 4, 1); }
+inline dim3 col_grid(int nx, int ny, int nz, int nodes) {
+  return dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 3) / 4), (unsigned)((nz + nodes - 1) / nodes));
+}
+
+template <typename R, int OP>
+void launch_stage_col(const StageArgs<R, SoA<R>> &a, bool per, bool hall, bool hod, int conv, cudaStream_t s);
+template <typename R, int OP>
+void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, cudaStream_t s);
+
+}  // namespace ieq

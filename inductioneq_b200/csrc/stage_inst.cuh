@@ -1,7 +1,7 @@
 // stage_inst.cuh -- instantiates the stage and curl kernels for one (REAL, operator) pair in
 // both field layouts.  Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so
 // the instantiations compile in parallel.
-#include "stage_kernel.cuh"
+#include "stage_col.cuh"
 
 namespace ieq {
 
@@ -59,6 +59,38 @@ void launch_curl<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a
                                             cudaStream_t s) {
   if (per) k_curl_rho<IEQ_R, SoA<IEQ_R>, IEQ_OP, true><<<grid, block, 0, s>>>(a);
   else k_curl_rho<IEQ_R, SoA<IEQ_R>, IEQ_OP, false><<<grid, block, 0, s>>>(a);
+}
+
+// the column kernels of the fused path (no first-order / adaptive dissipation)
+template <bool P, bool H>
+static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, dim3 g, dim3 b, cudaStream_t s) {
+  if (hod) {
+    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1><<<g, b, 0, s>>>(a);
+    else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0><<<g, b, 0, s>>>(a);
+  } else {
+    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1><<<g, b, 0, s>>>(a);
+    else k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0><<<g, b, 0, s>>>(a);
+  }
+}
+
+template <>
+void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
+                                     cudaStream_t s) {
+  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block();
+  if (per) {
+    if (hall) launch_col_ph<true, true>(a, hod, conv, g, b, s);
+    else launch_col_ph<true, false>(a, hod, conv, g, b, s);
+  } else {
+    if (hall) launch_col_ph<false, true>(a, hod, conv, g, b, s);
+    else launch_col_ph<false, false>(a, hod, conv, g, b, s);
+  }
+}
+
+template <>
+void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, cudaStream_t s) {
+  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, kCurlNodes), b = col_block();
+  if (per) k_curl_e<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
+  else k_curl_e<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
 }
 
 }  // namespace ieq

@@ -104,7 +104,8 @@ template <typename R, typename F = AoS<R>>
 struct StageArgs {
   Mesh m;
   F bk;                 // field the derivative is taken of
-  F J;                  // curl(B)/rho (Hall)
+  F J;                  // curl(B)/rho (Hall; the column kernel reads it on faces only)
+  F E;                  // (column kernel, Hall) J x B as (Jx By - Jy Bx, Jx Bz - Jz Bx, Jy Bz - Jz By)
   F u;
   F X, Y, Z;
   F out, out2;
@@ -251,6 +252,89 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R, F> &a, const int ii[3], co
   return acc;
 }
 
+// SAT surface terms on the faces of a non-periodic box (added into db)
+template <typename R, typename F, bool HALL>
+__device__ __forceinline__ void stage_sat(const StageArgs<R, F> &a, const int ii[3], const int nn[3], long long idx,
+                                          const V3<R> &Bm, const V3<R> &um, int conv, V3<R> &db) {
+  const int ix = ii[0], iy = ii[1], iz = ii[2], nx = nn[0], ny = nn[1], nz = nn[2];
+  const bool face = ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1;
+  if (face) {
+    if (HALL) {
+      // induction_Eq_surface.cl:35-81 (outflow, directional do-nothing)
+      const V3<R> Jm = ldf(a.J, idx);
+      const V3<R> tv = {(R)0.5 * um.x - Jm.x, (R)0.5 * um.y - Jm.y, (R)0.5 * um.z - Jm.z};
+      for (int ax = 0; ax < 3; ++ax) {
+        const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
+        if (!l && !r) continue;
+        const R tva = ax == 0 ? tv.x : (ax == 1 ? tv.y : tv.z);
+        const R Ba = ax == 0 ? Bm.x : (ax == 1 ? Bm.y : Bm.z);
+        const R c1 = (l && tva > (R)0 ? (R)-1 : (R)0) + (r && tva < (R)0 ? (R)1 : (R)0);
+        const R c2 = (l ? (R)-1 : (R)0) + (r ? (R)1 : (R)0);
+        const R f1 = c1 * tva, f2 = c2 * Ba;
+        db.x += a.sat_s[ax] * (f1 * Bm.x + f2 * Jm.x);
+        db.y += a.sat_s[ax] * (f1 * Bm.y + f2 * Jm.y);
+        db.z += a.sat_s[ax] * (f1 * Bm.z + f2 * Jm.z);
+      }
+    } else if (conv) {
+      // induction_Eq_surface.cl:7-33 (upwind inflow against b_boundary(t))
+      const R t = a.time[1];
+      const V3<R> bb = b_boundary<R>(a.tc, a.m, ix, iy, iz, t);
+      const V3<R> df = {Bm.x - bb.x, Bm.y - bb.y, Bm.z - bb.z};
+      for (int ax = 0; ax < 3; ++ax) {
+        const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
+        const R ua = ax == 0 ? um.x : (ax == 1 ? um.y : um.z);
+        const R c = (l && ua > (R)0 ? (R)-1 : (R)0) + (r && ua < (R)0 ? (R)1 : (R)0);
+        if (c == (R)0) continue;
+        const R f = (a.sat_s[ax] * c) * ua;
+        db.x += f * df.x; db.y += f * df.y; db.z += f * df.z;
+      }
+    }
+  }
+}
+
+// the stage update of the integrator (EpilogueMode) at one node
+template <typename R, typename F>
+__device__ __forceinline__ void stage_epilogue(const StageArgs<R, F> &a, long long idx, const V3<R> &db) {
+  V3<R> r;
+  switch (a.mode) {
+    case EP_X_PLUS_HF: {
+      const V3<R> X = ldf_plain(a.X, idx);
+      r = {X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
+      stf(a.out, idx, r);
+      break;
+    }
+    case EP_PX_QYHF: {
+      const V3<R> X = ldf_plain(a.X, idx), Y = ldf_plain(a.Y, idx);
+      r = {a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
+           a.p * X.z + a.q * (Y.z + a.h * db.z)};
+      stf(a.out, idx, r);
+      break;
+    }
+    case EP_HF:
+      stf(a.out, idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
+      break;
+    case EP_AX_HF: {
+      const V3<R> X = ldf_plain(a.X, idx);
+      stf(a.out, idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
+      break;
+    }
+    case EP_2N_FUSED:
+    case EP_2N_FUSED_FIRST: {
+      V3<R> t;
+      if (a.mode == EP_2N_FUSED) {
+        const V3<R> X = ldf_plain(a.X, idx);
+        t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
+      } else {
+        t = {a.h * db.x, a.h * db.y, a.h * db.z};
+      }
+      stf(a.out, idx, t);
+      const V3<R> Z = ldf_plain(a.Z, idx);
+      stf(a.out2, idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
+      break;
+    }
+  }
+}
+
 // DB and the stage update at one node (ix, iy, iz) inside the grid.
 template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV>
 __device__ __forceinline__ void stage_node(const StageArgs<R, F> &a, int ix, int iy, int iz) {
@@ -326,42 +410,7 @@ __device__ __forceinline__ void stage_node(const StageArgs<R, F> &a, int ix, int
         hod.x += s.SHo.x; hod.y += s.SHo.y; hod.z += s.SHo.z;
       }
     }
-    // ---- SAT surface terms on the faces of a non-periodic box
-    if (!PER) {
-      const bool face = ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1;
-      if (face) {
-        if (HALL) {
-          // induction_Eq_surface.cl:35-81 (outflow, directional do-nothing)
-          const V3<R> Jm = ldf(a.J, idx);
-          const V3<R> tv = {(R)0.5 * um.x - Jm.x, (R)0.5 * um.y - Jm.y, (R)0.5 * um.z - Jm.z};
-          for (int ax = 0; ax < 3; ++ax) {
-            const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
-            if (!l && !r) continue;
-            const R tva = ax == 0 ? tv.x : (ax == 1 ? tv.y : tv.z);
-            const R Ba = ax == 0 ? Bm.x : (ax == 1 ? Bm.y : Bm.z);
-            const R c1 = (l && tva > (R)0 ? (R)-1 : (R)0) + (r && tva < (R)0 ? (R)1 : (R)0);
-            const R c2 = (l ? (R)-1 : (R)0) + (r ? (R)1 : (R)0);
-            const R f1 = c1 * tva, f2 = c2 * Ba;
-            db.x += a.sat_s[ax] * (f1 * Bm.x + f2 * Jm.x);
-            db.y += a.sat_s[ax] * (f1 * Bm.y + f2 * Jm.y);
-            db.z += a.sat_s[ax] * (f1 * Bm.z + f2 * Jm.z);
-          }
-        } else if (conv) {
-          // induction_Eq_surface.cl:7-33 (upwind inflow against b_boundary(t))
-          const R t = a.time[1];
-          const V3<R> bb = b_boundary<R>(a.tc, a.m, ix, iy, iz, t);
-          const V3<R> df = {Bm.x - bb.x, Bm.y - bb.y, Bm.z - bb.z};
-          for (int ax = 0; ax < 3; ++ax) {
-            const bool l = ii[ax] == 0, r = ii[ax] == nn[ax] - 1;
-            const R ua = ax == 0 ? um.x : (ax == 1 ? um.y : um.z);
-            const R c = (l && ua > (R)0 ? (R)-1 : (R)0) + (r && ua < (R)0 ? (R)1 : (R)0);
-            if (c == (R)0) continue;
-            const R f = (a.sat_s[ax] * c) * ua;
-            db.x += f * df.x; db.y += f * df.y; db.z += f * df.z;
-          }
-        }
-      }
-    }
+    if (!PER) stage_sat<R, F, HALL>(a, ii, nn, idx, Bm, um, conv, db);
     if (HOD) {
       db.x += a.hod_factor * hod.x;
       db.y += a.hod_factor * hod.y;
@@ -371,55 +420,14 @@ __device__ __forceinline__ void stage_node(const StageArgs<R, F> &a, int ix, int
       const V3<R> ds = fo_ad_dissipation<R, F, OP, PER>(a, ii, nn, st, idx, Bm, um);
       db.x += ds.x; db.y += ds.y; db.z += ds.z;
     }
-    // ---- stage update
-    V3<R> r;
-    switch (a.mode) {
-      case EP_X_PLUS_HF: {
-        const V3<R> X = ldf_plain(a.X, idx);
-        r = {X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
-        stf(a.out, idx, r);
-        break;
-      }
-      case EP_PX_QYHF: {
-        const V3<R> X = ldf_plain(a.X, idx), Y = ldf_plain(a.Y, idx);
-        r = {a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
-             a.p * X.z + a.q * (Y.z + a.h * db.z)};
-        stf(a.out, idx, r);
-        break;
-      }
-      case EP_HF:
-        stf(a.out, idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
-        break;
-      case EP_AX_HF: {
-        const V3<R> X = ldf_plain(a.X, idx);
-        stf(a.out, idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
-        break;
-      }
-      case EP_2N_FUSED:
-      case EP_2N_FUSED_FIRST: {
-        V3<R> t;
-        if (a.mode == EP_2N_FUSED) {
-          const V3<R> X = ldf_plain(a.X, idx);
-          t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
-        } else {
-          t = {a.h * db.x, a.h * db.y, a.h * db.z};
-        }
-        stf(a.out, idx, t);
-        const V3<R> Z = ldf_plain(a.Z, idx);
-        stf(a.out2, idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
-        break;
-      }
-    }
+    stage_epilogue<R, F>(a, idx, db);
   }
 }
 
-template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV = -1>
-__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R, F> a) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
-  if (ix < a.m.nx && iy < a.m.ny && iz < a.m.nz) stage_node<R, F, OP, PER, HALL, DISS, CONV>(a, ix, iy, iz);
-  // ---- time bookkeeping of the folded "a"/calc_time kernels, done by the last block
+// time bookkeeping of the folded "a"/calc_time kernels, done by the last block to finish
+// (every thread of the block must call this)
+template <typename R, typename F>
+__device__ __forceinline__ void stage_time_post(const StageArgs<R, F> &a) {
   if (a.tpost != TP_NONE) {
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
@@ -441,6 +449,15 @@ __global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs
   }
 }
 
+template <typename R, typename F, int OP, bool PER, bool HALL, int DISS, int CONV = -1>
+__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs<R, F> a) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix < a.m.nx && iy < a.m.ny && iz < a.m.nz) stage_node<R, F, OP, PER, HALL, DISS, CONV>(a, ix, iy, iz);
+  stage_time_post(a);
+}
+
 // curl(b)/rho (kernel_time_integrator.cl:136-208 via SBP_operator.cl:126-135), with the
 // same interior/boundary row split; diff_* divide by (REAL)DX as the reference does.
 template <typename R, typename F = AoS<R>>
@@ -449,6 +466,7 @@ struct CurlArgs {
   F b;
   const R *rho;       // nullptr: plain curl (kernel_operator.cl:158 calc_curl)
   F out;
+  F jface;      // (k_curl_e) J on the faces of a non-periodic box
   const Tables<R> *tab;
   R dR[3];
   R inv_d[3];   // (REAL)(1.0/DX) ...
