@@ -305,7 +305,7 @@ def form_precision(dev, n=128, steps=20):
 
 
 def form_adjoint(dev, n=64, t_final=0.2, every=10, n_dirs=20):
-    """Hall periodic (include/hall_periodic.h) 64^3, FP64, 4th order, variable u, SSPRK33 at CFL 2/N
+    """Hall periodic (include/hall_periodic.h) 64^3, FP64, 4th order, variable u, SSPRK33 at CFL 1/N
     to t = 0.2: gradient of J = 1/2 ||B(T) - B_tgt||_M^2 (B_tgt = exact(T) + seeded N(0, 1e-3)) with
     respect to B0 by the checkpointed adjoint, checked against Richardson-extrapolated central
     differences along seeded unit directions."""
@@ -329,7 +329,10 @@ def form_adjoint(dev, n=64, t_final=0.2, every=10, n_dirs=20):
     umax = float(np.sqrt((ctx.get_vec(u)[:, :3] ** 2).sum(1)).max())
     ctx.close()
     dx = hp / n
-    dt = (2.0 / n) * dx / umax                      # initialize.m:93-99 with CFL 2/N
+    # initialize.m:93-99 with CFL 1/N: the reference example pairs CFL 2/N with
+    # CarpenterKennedy2N54 (compute_error_hall_periodic.m:51-57); SSPRK33, whose stability
+    # interval on the imaginary axis is shorter, blows up at CFL 2/N on 64^3
+    dt = (1.0 / n) * dx / umax
     steps = math.ceil(t_final / dt)
     dt = t_final / steps
     ctx = mk(dt)
@@ -401,6 +404,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 / batched / precision lines")
+    ap.add_argument("--stage-kernel", choices=("AUTO", "COLUMN", "BRICK"), default="AUTO",
+                    help="kernels of the fused stages (IEQ_STAGE_KERNEL)")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -432,6 +437,7 @@ def main() -> None:
     dev = local_rank
     torch.cuda.set_device(dev)
     m = maps()
+    m.I_Tech["stage_kernel"] = a.stage_kernel
     ctx = m.context(device=dev)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     nn = ctx.n
@@ -540,7 +546,8 @@ def main() -> None:
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     achieved = STAGE_BYTES_PER_NODE * nn / stage_avg / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_stage_col<double, 6th classical, periodic, Hall, HOD, u=0> (fused CK2N54 a+b)",
+    roofline = {"bound": "hbm", "kernel": ("k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col") +
+                "<double, 6th classical, periodic, Hall, HOD, u=0> (fused CK2N54 a+b)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_src, "traffic": None,
                 "algorithmic_bytes_per_node": STAGE_BYTES_PER_NODE, "nodes_per_launch": nn,
@@ -557,6 +564,7 @@ def main() -> None:
         "ms_per_step": t_max / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (analytic whistler wave)",
         "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "rk_steps_per_step": NUM_STEPS_FULL,
+                   "stage_kernels": a.stage_kernel,
                    "stages_per_rk_step": STAGES, "step": "one full solve to t=0.5 (260 RK steps)",
                    "l2": L2_NOTE, "replicas": world},
         "e2e": {"value": e2e_value, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -3,12 +3,17 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "ieq_host.h"
 #include "misc_kernels.cuh"
-#include "stage_col.cuh"
+#include "stage_brick.cuh"
+
+namespace ieq {
+void free_brick_maps(ieq_ctx *c);   // api_fused.inc
+}
 
 using namespace ieq;
 
@@ -242,6 +247,36 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
     case 3: launch_curl_e<R, 3>(a, per, c->stream); break;
     case 4: launch_curl_e<R, 4>(a, per, c->stream); break;
     case 5: launch_curl_e<R, 5>(a, per, c->stream); break;
+  }
+}
+
+template <typename R>
+void launch_stage_brick_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, const TmaStageMaps &maps) {
+  const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
+  int *err = c->d_flag + 2;
+  switch (c->op_id) {
+    case 0: launch_stage_brick<R, 0>(a, maps, err, per, hall, hod, c->stream); break;
+    case 1: launch_stage_brick<R, 1>(a, maps, err, per, hall, hod, c->stream); break;
+    case 2: launch_stage_brick<R, 2>(a, maps, err, per, hall, hod, c->stream); break;
+    case 3: launch_stage_brick<R, 3>(a, maps, err, per, hall, hod, c->stream); break;
+    case 4: launch_stage_brick<R, 4>(a, maps, err, per, hall, hod, c->stream); break;
+    case 5: launch_stage_brick<R, 5>(a, maps, err, per, hall, hod, c->stream); break;
+  }
+}
+
+template <typename R>
+void launch_curl_brick_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jface, const TmaStageMaps &maps) {
+  CurlArgs<R, SoA<R>> a = curl_args<R, SoA<R>>(c, b, rho, E);
+  a.jface = jface;
+  const bool per = c->s.periodic;
+  int *err = c->d_flag + 2;
+  switch (c->op_id) {
+    case 0: launch_curl_brick<R, 0>(a, maps, err, per, c->stream); break;
+    case 1: launch_curl_brick<R, 1>(a, maps, err, per, c->stream); break;
+    case 2: launch_curl_brick<R, 2>(a, maps, err, per, c->stream); break;
+    case 3: launch_curl_brick<R, 3>(a, maps, err, per, c->stream); break;
+    case 4: launch_curl_brick<R, 4>(a, maps, err, per, c->stream); break;
+    case 5: launch_curl_brick<R, 5>(a, maps, err, per, c->stream); break;
   }
 }
 
@@ -717,6 +752,7 @@ ieq_status ieq_create(ieq_ctx **out, const char *settings, const char *const *pa
   if (st == IEQ_OK) cuda(cudaMalloc(&c->d_counter, 64 * sizeof(unsigned)), "cudaMalloc");
   if (st == IEQ_OK) cuda(cudaMemset(c->d_counter, 0, 64 * sizeof(unsigned)), "cudaMemset");
   if (st == IEQ_OK) cuda(cudaMalloc(&c->d_flag, 64 * sizeof(int)), "cudaMalloc");
+  if (st == IEQ_OK) cuda(cudaMemset(c->d_flag, 0, 64 * sizeof(int)), "cudaMemset");
   if (st == IEQ_OK) cuda(cudaMalloc(&c->d_cg, sizeof(CgState)), "cudaMalloc");
   if (st == IEQ_OK) cuda(cudaEventCreate(&c->ev0), "cudaEventCreate");
   if (st == IEQ_OK) cuda(cudaEventCreate(&c->ev1), "cudaEventCreate");
@@ -736,6 +772,7 @@ void ieq_destroy(ieq_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  ieq::free_brick_maps(c);
   for (auto &kv : c->graphs) {
     if (kv.second.exec1) cudaGraphExecDestroy(kv.second.exec1);
     if (kv.second.exec2) cudaGraphExecDestroy(kv.second.exec2);

@@ -37,6 +37,10 @@ struct Settings {
   double omega = 1.0;
   std::string integrator;
   bool variable_u = false;
+  // kernels of the fused time stepping (IEQ_STAGE_KERNEL): 0 AUTO (the column kernels,
+  // measured fastest on B200), 1 COLUMN, 2 NODE (the per-node J-based kernels), 3 BRICK
+  // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN)
+  int stage_kernel = 0;
 };
 
 // parse helpers (settings.cpp)
@@ -86,6 +90,7 @@ struct ieq_ctx {
   int cg_hist_len = 0;
   void *d_pingpong = nullptr;      // (unused)
   void *d_soa = nullptr;           // structure-of-arrays state of the fused time stepping
+  void *brick_maps = nullptr;      // tensor maps of that state for the TMA brick kernels (host)
   std::set<void *> allocs;
   // fused time-step graphs keyed by the argument pointers
   struct GraphEntry {

@@ -119,6 +119,12 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
       s.integrator = val;
     } else if (key == "IEQ_VARIABLE_U") {
       s.variable_u = val != "0";
+    } else if (key == "IEQ_STAGE_KERNEL") {
+      if (val == "AUTO") s.stage_kernel = 0;
+      else if (val == "COLUMN") s.stage_kernel = 1;
+      else if (val == "NODE") s.stage_kernel = 2;
+      else if (val == "BRICK") s.stage_kernel = 3;
+      else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE or BRICK"; return false; }
     } else if (key == "USE_HALL") {
       s.hall = true;
     } else if (key == "USE_PERIODIC") {

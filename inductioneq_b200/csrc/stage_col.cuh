@@ -31,6 +31,17 @@ namespace ieq {
 #ifndef IEQ_CURL_NODES
 #define IEQ_CURL_NODES 1
 #endif
+#ifndef IEQ_COL_BX
+#define IEQ_COL_BX 32
+#endif
+#ifndef IEQ_COL_BY
+#define IEQ_COL_BY 4
+#endif
+#ifndef IEQ_COL_BZ
+#define IEQ_COL_BZ 1
+#endif
+constexpr int kColBX = IEQ_COL_BX, kColBY = IEQ_COL_BY, kColBZ = IEQ_COL_BZ;
+constexpr int kColThreads = kColBX * kColBY * kColBZ;
 constexpr int kColNodes = IEQ_COL_NODES;     // nodes per thread along z (stage kernel)
 constexpr int kCurlNodes = IEQ_CURL_NODES;   // nodes per thread along z (curl kernel)
 // the convection terms keep twelve sums per node and axis: one node per thread there
@@ -160,7 +171,7 @@ __device__ __forceinline__ void col_combine(const StageArgs<R, SoA<R>> &a, int a
 }
 
 template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
-__global__ void __launch_bounds__(128, CONV ? 2 : IEQ_COL_MIN_BLOCKS) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+__global__ void __launch_bounds__(kColThreads, CONV ? 256 / kColThreads : IEQ_COL_MIN_BLOCKS * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
   constexpr int NZ = col_nodes(CONV);
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
@@ -271,7 +282,7 @@ __global__ void __launch_bounds__(128, CONV ? 2 : IEQ_COL_MIN_BLOCKS) k_stage_co
 
 // J = curl(B)/rho and E = J x B, two nodes per thread along z (see the file comment)
 template <typename R, int OP, bool PER>
-__global__ void __launch_bounds__(128) k_curl_e(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+__global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
   constexpr int NZ = kCurlNodes;
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
@@ -385,10 +396,13 @@ __global__ void __launch_bounds__(128) k_curl_e(const __grid_constant__ CurlArgs
   }
 }
 
-// launch shape of the column kernels: 32 x 4 threads, each `nodes` nodes in z
-inline dim3 col_block() { return dim3(32, 4, 1); }
+// launch shape of the column kernels: kColBX x kColBY x kColBZ threads (kColThreads), each
+// `nodes` nodes in z
+inline dim3 col_block() { return dim3(kColBX, kColBY, kColBZ); }
 inline dim3 col_grid(int nx, int ny, int nz, int nodes) {
-  return dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 3) / 4), (unsigned)((nz + nodes - 1) / nodes));
+  const int zb = kColBZ * nodes;
+  return dim3((unsigned)((nx + kColBX - 1) / kColBX), (unsigned)((ny + kColBY - 1) / kColBY),
+              (unsigned)((nz + zb - 1) / zb));
 }
 
 template <typename R, int OP>

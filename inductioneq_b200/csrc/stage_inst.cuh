@@ -1,7 +1,7 @@
 // stage_inst.cuh -- instantiates the stage and curl kernels for one (REAL, operator) pair in
 // both field layouts.  Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so
 // the instantiations compile in parallel.
-#include "stage_col.cuh"
+#include "stage_brick.cuh"
 
 namespace ieq {
 
@@ -91,6 +91,60 @@ void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per
   const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, kCurlNodes), b = col_block();
   if (per) k_curl_e<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
   else k_curl_e<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
+}
+
+// the TMA brick kernels (u = 0 stages); the dynamic shared memory limit of each
+// instantiation is raised once, before its first launch
+template <bool P, bool H, bool D>
+static void launch_brick_phd(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, const TmaStageMaps &maps, int *err,
+                             cudaStream_t s) {
+  constexpr int smem = brick_smem_bytes<IEQ_R>((H ? 1 : 0) + (D ? 1 : 0));
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_stage_brick<IEQ_R, IEQ_OP, P, H, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_stage_brick<IEQ_R, IEQ_OP, P, H, D>
+      <<<brick_grid(a.m.nx, a.m.ny, a.m.nz), kBrickThreads, smem, s>>>(a, maps, err);
+}
+
+template <>
+void launch_stage_brick<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, const TmaStageMaps &maps, int *err,
+                                       bool per, bool hall, bool hod, cudaStream_t s) {
+  if (per) {
+    if (hall) {
+      if (hod) launch_brick_phd<true, true, true>(a, maps, err, s);
+      else launch_brick_phd<true, true, false>(a, maps, err, s);
+    } else if (hod) {
+      launch_brick_phd<true, false, true>(a, maps, err, s);
+    }
+  } else {
+    if (hall) {
+      if (hod) launch_brick_phd<false, true, true>(a, maps, err, s);
+      else launch_brick_phd<false, true, false>(a, maps, err, s);
+    } else if (hod) {
+      launch_brick_phd<false, false, true>(a, maps, err, s);
+    }
+  }
+}
+
+template <bool P>
+static void launch_curl_brick_p(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, const TmaStageMaps &maps, int *err,
+                                cudaStream_t s) {
+  constexpr int smem = brick_smem_bytes<IEQ_R>(1);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_curl_brick<IEQ_R, IEQ_OP, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_curl_brick<IEQ_R, IEQ_OP, P><<<brick_grid(a.m.nx, a.m.ny, a.m.nz), kBrickThreads, smem, s>>>(a, maps, err);
+}
+
+template <>
+void launch_curl_brick<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, const TmaStageMaps &maps, int *err,
+                                      bool per, cudaStream_t s) {
+  if (per) launch_curl_brick_p<true>(a, maps, err, s);
+  else launch_curl_brick_p<false>(a, maps, err, s);
 }
 
 }  // namespace ieq

@@ -292,47 +292,72 @@ __device__ __forceinline__ void stage_sat(const StageArgs<R, F> &a, const int ii
   }
 }
 
-// the stage update of the integrator (EpilogueMode) at one node
+// the stage update of the integrator (EpilogueMode) at one node, split into the loads of
+// the fields it combines (which do not depend on DB, so a kernel may issue them early) and
+// the arithmetic and stores
+template <typename R>
+struct EpIn {
+  V3<R> X, Y;   // X; Y (EP_PX_QYHF) or Z (the fused 2N modes)
+};
+
 template <typename R, typename F>
-__device__ __forceinline__ void stage_epilogue(const StageArgs<R, F> &a, long long idx, const V3<R> &db) {
-  V3<R> r;
+__device__ __forceinline__ EpIn<R> epilogue_load(const StageArgs<R, F> &a, long long idx) {
+  EpIn<R> e = {{0, 0, 0}, {0, 0, 0}};
   switch (a.mode) {
-    case EP_X_PLUS_HF: {
-      const V3<R> X = ldf_plain(a.X, idx);
-      r = {X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
-      stf(a.out, idx, r);
+    case EP_X_PLUS_HF:
+    case EP_AX_HF:
+      e.X = ldf_plain(a.X, idx);
       break;
-    }
-    case EP_PX_QYHF: {
-      const V3<R> X = ldf_plain(a.X, idx), Y = ldf_plain(a.Y, idx);
-      r = {a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
-           a.p * X.z + a.q * (Y.z + a.h * db.z)};
-      stf(a.out, idx, r);
+    case EP_PX_QYHF:
+      e.X = ldf_plain(a.X, idx);
+      e.Y = ldf_plain(a.Y, idx);
       break;
-    }
+    case EP_2N_FUSED:
+      e.X = ldf_plain(a.X, idx);
+      e.Y = ldf_plain(a.Z, idx);
+      break;
+    case EP_2N_FUSED_FIRST:
+      e.Y = ldf_plain(a.Z, idx);
+      break;
+    default:
+      break;
+  }
+  return e;
+}
+
+template <typename R, typename F>
+__device__ __forceinline__ void epilogue_store(const StageArgs<R, F> &a, long long idx, const V3<R> &db,
+                                               const EpIn<R> &e) {
+  const V3<R> &X = e.X, &Y = e.Y;
+  switch (a.mode) {
+    case EP_X_PLUS_HF:
+      stf(a.out, idx, V3<R>{X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z});
+      break;
+    case EP_PX_QYHF:
+      stf(a.out, idx, V3<R>{a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
+                            a.p * X.z + a.q * (Y.z + a.h * db.z)});
+      break;
     case EP_HF:
       stf(a.out, idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
       break;
-    case EP_AX_HF: {
-      const V3<R> X = ldf_plain(a.X, idx);
+    case EP_AX_HF:
       stf(a.out, idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
       break;
-    }
     case EP_2N_FUSED:
     case EP_2N_FUSED_FIRST: {
       V3<R> t;
-      if (a.mode == EP_2N_FUSED) {
-        const V3<R> X = ldf_plain(a.X, idx);
-        t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
-      } else {
-        t = {a.h * db.x, a.h * db.y, a.h * db.z};
-      }
+      if (a.mode == EP_2N_FUSED) t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
+      else t = {a.h * db.x, a.h * db.y, a.h * db.z};
       stf(a.out, idx, t);
-      const V3<R> Z = ldf_plain(a.Z, idx);
-      stf(a.out2, idx, V3<R>{Z.x + a.Bc * t.x, Z.y + a.Bc * t.y, Z.z + a.Bc * t.z});
+      stf(a.out2, idx, V3<R>{Y.x + a.Bc * t.x, Y.y + a.Bc * t.y, Y.z + a.Bc * t.z});
       break;
     }
   }
+}
+
+template <typename R, typename F>
+__device__ __forceinline__ void stage_epilogue(const StageArgs<R, F> &a, long long idx, const V3<R> &db) {
+  epilogue_store(a, idx, db, epilogue_load(a, idx));
 }
 
 // DB and the stage update at one node (ix, iy, iz) inside the grid.

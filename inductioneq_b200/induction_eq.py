@@ -104,6 +104,8 @@ class Maps:
         if self.I_RunOps.get("variable_u"):
             s += " -DIEQ_VARIABLE_U=1"
         s += f" -DTC_OMEGA={self.tc_omega:.16e}"
+        if self.I_Tech.get("stage_kernel", "AUTO") != "AUTO":
+            s += f" -DIEQ_STAGE_KERNEL={self.I_Tech['stage_kernel']}"
         return s
 
     def kernel_path_list(self) -> list[str]:
