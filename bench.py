@@ -554,10 +554,17 @@ def main() -> None:
                 "avg_launch_ms": stage_avg * 1e3, "curl_kernel_avg_ms": curl_avg * 1e3,
                 "note": "CUDA events around a graph of 20 back-to-back launches of each kernel of one step "
                         "(L2 warm, as inside a solve)"}
-    traffic_file = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
-    if os.path.isfile(traffic_file):
-        with open(traffic_file) as f:
-            roofline["traffic"] = json.load(f).get("bytes_per_launch")
+    # DRAM bytes (read + write) of one launch of the stage kernel, from the ncu capture
+    # summarised in profiles/ ("traffic_bytes_per_launch: N" line of the kernel's summary)
+    kname = "k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col"
+    summary = os.path.join(ROOT, "profiles", f"{kname}_hall6_64cubed.md")
+    if os.path.isfile(summary):
+        with open(summary) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    roofline["traffic"] = int(line.split(":", 1)[1].strip())
+                    roofline["traffic_note"] = ("ncu capture with caches flushed before the launch: the inputs b1 and "
+                                                "E come from DRAM, the writes stay in L2")
 
     out = {
         "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
