@@ -167,9 +167,17 @@ void *ieq_batch_stream(ieq_batch *batch);
 ieq_status ieq_batch_set_tile(ieq_batch *batch, int solve, int tx, int ty, int tz);
 /* fields[5*i + 0..4] = solve i's b, b2, b3, u, time (device pointers, reference layout) */
 ieq_status ieq_batch_bind(ieq_batch *batch, void *const *fields);
-/* num_steps steps of all bound solves; persistent = 0 launches one kernel per stage instead
- * of one persistent kernel.  IEQ_ERR_TIMEOUT if a bounded grid barrier gave up.  Syncs. */
-ieq_status ieq_batch_run(ieq_batch *batch, int num_steps, int persistent);
+/* num_steps steps of all bound solves, captured in one CUDA graph, by
+ *   mode IEQ_BATCH_PERSISTENT (1): one persistent kernel over the tile queue, stages
+ *     separated by a bounded software grid barrier;
+ *   mode IEQ_BATCH_STAGES (0): one kernel over the tile queue per stage;
+ *   mode IEQ_BATCH_BRANCHES (2): one graph branch per solve (its fused column kernels on its
+ *     own stream), the branches running concurrently.
+ * IEQ_ERR_TIMEOUT if a bounded grid barrier gave up.  Syncs. */
+#define IEQ_BATCH_STAGES 0
+#define IEQ_BATCH_PERSISTENT 1
+#define IEQ_BATCH_BRANCHES 2
+ieq_status ieq_batch_run(ieq_batch *batch, int num_steps, int mode);
 /* copy the solves' b, b2, b3 back into the bound fields */
 ieq_status ieq_batch_unbind(ieq_batch *batch);
 long long ieq_batch_total_tiles(const ieq_batch *batch);

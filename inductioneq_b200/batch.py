@@ -109,8 +109,14 @@ class Batch:
         arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
         self._check(self.lib.ieq_batch_bind(self.h, arr))
 
-    def run(self, steps: int, persistent: bool = True):
-        self._check(self.lib.ieq_batch_run(self.h, int(steps), 1 if persistent else 0))
+    MODES = {"stages": 0, "persistent": 1, "branches": 2}
+
+    def run(self, steps: int, persistent: bool = True, mode: str | None = None):
+        """Advance every bound solve `steps` SSPRK33 steps: mode "persistent" (one persistent
+        kernel over the tile queue), "stages" (one tile-queue kernel per stage) or "branches"
+        (one graph branch per solve); `persistent` picks between the first two."""
+        m = self.MODES[mode] if mode is not None else (1 if persistent else 0)
+        self._check(self.lib.ieq_batch_run(self.h, int(steps), m))
 
     def unbind(self):
         self._check(self.lib.ieq_batch_unbind(self.h))

@@ -34,6 +34,11 @@ struct BatchSync {
   int pad;
 };
 
+// resident blocks of 256 threads per SM the batched kernels are compiled for
+#ifndef IEQ_BATCH_MIN_BLOCKS
+#define IEQ_BATCH_MIN_BLOCKS 2
+#endif
+
 constexpr long long kBarrierSpinLimit = 20000000;   // x 64 ns nanosleep: about 1.3 s
 
 // bounded grid barrier; the last block to arrive runs `last` before releasing the others
@@ -129,7 +134,7 @@ __device__ void batch_times(const BatchSolveDesc *descs, int ns, int stage) {
   __threadfence();
 }
 
-__global__ void __launch_bounds__(256) k_batch_persistent(const BatchSolveDesc *descs, int ns, long long ntiles,
+__global__ void __launch_bounds__(256, IEQ_BATCH_MIN_BLOCKS) k_batch_persistent(const BatchSolveDesc *descs, int ns, long long ntiles,
                                                           int nsteps, BatchSync *sync) {
   __shared__ StageArgs<double, SoAcg<double>> sa;
   __shared__ BatchSolveDesc sd;
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(256) k_batch_persistent(const BatchSolveDesc *
 }
 
 // the same stage as an ordinary launch (one block per tile); the last block does the times
-__global__ void __launch_bounds__(256) k_batch_stage(const BatchSolveDesc *descs, int ns, long long ntiles, int stage,
+__global__ void __launch_bounds__(256, IEQ_BATCH_MIN_BLOCKS) k_batch_stage(const BatchSolveDesc *descs, int ns, long long ntiles, int stage,
                                                      BatchSync *sync) {
   __shared__ StageArgs<double, SoA<double>> sa;
   __shared__ BatchSolveDesc sd;
@@ -175,9 +180,11 @@ struct ieq_batch {
   std::string err;
   std::vector<int> tiles;   // tx, ty, tz per solve
   cudaGraphExec_t graph = nullptr;
-  int graph_steps = -1, graph_persistent = -1;
+  int graph_steps = -1, graph_persistent = -1;   // graph_persistent: the mode of the graph
   int grid = 0;
   std::vector<void *> bound;
+  cudaEvent_t fork = nullptr;          // IEQ_BATCH_BRANCHES: fork/join of the solves' streams
+  std::vector<cudaEvent_t> join;
 };
 
 // from api.cu / api_fused.inc
@@ -186,6 +193,7 @@ template <typename R, typename F>
 StageArgs<R, F> stage_args_for_batch(ieq_ctx *c);
 ieq_status batch_enter(ieq_ctx *c, void *b, void *b2, void *b3, void *u, double **soa_base, long long *stride);
 ieq_status batch_leave(ieq_ctx *c, void *b, void *b2, void *b3);
+ieq_status batch_enqueue_steps(ieq_ctx *c, int steps, double *time);
 }  // namespace ieq
 
 static ieq_status bfail(ieq_batch *b, ieq_status st, const std::string &m) {
@@ -221,7 +229,10 @@ ieq_status ieq_batch_create(ieq_batch **out, ieq_ctx *const *solves, int n) {
   }
   b->device = solves[0]->device;
   cudaSetDevice(b->device);
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  b->join.assign(n, nullptr);
+  bool ev = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < n && ev; ++i) ev = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ev || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&b->d_desc, n * sizeof(BatchSolveDesc)) != cudaSuccess ||
       cudaMalloc(&b->d_sync, sizeof(BatchSync)) != cudaSuccess ||
       cudaMemset(b->d_sync, 0, sizeof(BatchSync)) != cudaSuccess) {
@@ -241,6 +252,9 @@ void ieq_batch_destroy(ieq_batch *b) {
   if (b->d_desc) cudaFree(b->d_desc);
   if (b->d_sync) cudaFree(b->d_sync);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
   delete b;
 }
 
@@ -329,11 +343,11 @@ ieq_status ieq_batch_bind(ieq_batch *b, void *const *fields) {
 // persistent launch (stages separated by the bounded grid barrier); 0: one launch per stage.
 // Either is captured once into a CUDA graph and replayed.  Returns IEQ_ERR_TIMEOUT if a
 // grid barrier gave up (blocks not co-resident).  Synchronises.
-ieq_status ieq_batch_run(ieq_batch *b, int num_steps, int persistent) {
-  if (!b || num_steps < 0 || b->ntiles == 0) return IEQ_ERR_ARG;
+ieq_status ieq_batch_run(ieq_batch *b, int num_steps, int mode) {
+  if (!b || num_steps < 0 || b->ntiles == 0 || mode < 0 || mode > 2) return IEQ_ERR_ARG;
   if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "cudaSetDevice");
   const int n = (int)b->solves.size();
-  if (!b->graph || b->graph_steps != num_steps || b->graph_persistent != persistent) {
+  if (!b->graph || b->graph_steps != num_steps || b->graph_persistent != mode) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     int per_sm = 0, nsm = 0;
@@ -342,21 +356,44 @@ ieq_status ieq_batch_run(ieq_batch *b, int num_steps, int persistent) {
     const long long resident = (long long)per_sm * nsm;
     b->grid = (int)(resident < b->ntiles ? resident : b->ntiles);
     if (b->grid < 1) return bfail(b, IEQ_ERR_CUDA, "no resident blocks for the persistent kernel");
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
       return bfail(b, IEQ_ERR_CUDA, "capture");
-    if (persistent) {
+    if (mode == IEQ_BATCH_BRANCHES) {
+      // one branch per solve: fork onto the solves' streams, join back
+      ieq_status st = IEQ_OK;
+      if (cudaEventRecord(b->fork, b->stream) != cudaSuccess) st = IEQ_ERR_CUDA;
+      for (int i = 0; i < n && st == IEQ_OK; ++i) {
+        ieq_ctx *c = b->solves[i];
+        if (cudaStreamWaitEvent(c->stream, b->fork, 0) != cudaSuccess) st = IEQ_ERR_CUDA;
+        if (st == IEQ_OK) st = batch_enqueue_steps(c, num_steps, b->host[i].time);
+        if (st == IEQ_OK && (cudaEventRecord(b->join[i], c->stream) != cudaSuccess ||
+                             cudaStreamWaitEvent(b->stream, b->join[i], 0) != cudaSuccess))
+          st = IEQ_ERR_CUDA;
+      }
+      cudaStreamEndCapture(b->stream, &g);
+      if (st != IEQ_OK) {
+        if (g) cudaGraphDestroy(g);
+        return bfail(b, st, "branch capture");
+      }
+      if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "instantiate");
+      cudaGraphDestroy(g);
+      b->graph_steps = num_steps;
+      b->graph_persistent = mode;
+    } else if (mode == IEQ_BATCH_PERSISTENT) {
       k_batch_persistent<<<b->grid, 256, 0, b->stream>>>(b->d_desc, n, b->ntiles, num_steps, b->d_sync);
     } else {
       for (int step = 0; step < num_steps; ++step)
         for (int k = 0; k < 3; ++k)
           k_batch_stage<<<(unsigned)b->ntiles, 256, 0, b->stream>>>(b->d_desc, n, b->ntiles, k, b->d_sync);
     }
-    if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "capture end");
-    if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "instantiate");
-    cudaGraphDestroy(g);
-    b->graph_steps = num_steps;
-    b->graph_persistent = persistent;
+    if (mode != IEQ_BATCH_BRANCHES) {
+      if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "capture end");
+      if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "instantiate");
+      cudaGraphDestroy(g);
+      b->graph_steps = num_steps;
+      b->graph_persistent = mode;
+    }
   }
   if (num_steps > 0 && cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "launch");
   BatchSync hs{};

@@ -28,6 +28,9 @@ namespace ieq {
 #ifndef IEQ_COL_MIN_BLOCKS
 #define IEQ_COL_MIN_BLOCKS 8
 #endif
+#ifndef IEQ_COL_CONV_MIN_BLOCKS
+#define IEQ_COL_CONV_MIN_BLOCKS 8
+#endif
 #ifndef IEQ_CURL_NODES
 #define IEQ_CURL_NODES 1
 #endif
@@ -88,8 +91,8 @@ __device__ __forceinline__ void col_acc(ColSums<R> &s, int ax, int need, R cD, R
   }
 }
 
-template <typename R, bool HALL, bool HOD, int CONV>
-__device__ __forceinline__ void col_load(const StageArgs<R, SoA<R>> &a, int ax, long long j, V3<R> &B, V3<R> &U,
+template <typename R, bool HALL, bool HOD, int CONV, typename F = SoA<R>>
+__device__ __forceinline__ void col_load(const StageArgs<R, F> &a, int ax, long long j, V3<R> &B, V3<R> &U,
                                          R &e1, R &e2) {
   if (CONV || HOD) B = ldf(a.bk, j);
   if (CONV) U = ldf(a.u, j);
@@ -99,10 +102,12 @@ __device__ __forceinline__ void col_load(const StageArgs<R, SoA<R>> &a, int ax, 
   }
 }
 
-// the sums of one axis at one node (interior row, periodic wrap or SBP boundary row)
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
-__device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, SoA<R>> &a, int ax, int i, int n,
+// the sums of one axis at one node (interior row, periodic wrap or SBP boundary row);
+// NEED >= 0 fixes the flux-form mask (StageArgs::need) at compile time
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, typename F = SoA<R>, int NEED = -1>
+__device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, F> &a, int ax, int i, int n,
                                          long long idx, long long st, const V3<R> &Bm) {
+  const int need = NEED >= 0 ? NEED : a.need;
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
   const V3<R> zero = {0, 0, 0};
@@ -119,8 +124,8 @@ __device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, SoA<R
       const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st : idx + (long long)o * st;
       V3<R> B = zero, U = zero;
       R e1 = 0, e2 = 0;
-      col_load<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
-      col_acc<R, HALL, HOD, CONV>(s, ax, a.need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
+      col_load<R, HALL, HOD, CONV, F>(a, ax, j, B, U, e1, e2);
+      col_acc<R, HALL, HOD, CONV>(s, ax, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
     }
   } else {
     for (int o = -RB; o <= RB; ++o) {
@@ -130,15 +135,15 @@ __device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, SoA<R
       const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st;
       V3<R> B = zero, U = zero;
       R e1 = 0, e2 = 0;
-      col_load<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
-      col_acc<R, HALL, HOD, CONV>(s, ax, a.need, cD, cH, cD != (R)0, cH != (R)0, B, U, e1, e2);
+      col_load<R, HALL, HOD, CONV, F>(a, ax, j, B, U, e1, e2);
+      col_acc<R, HALL, HOD, CONV>(s, ax, need, cD, cH, cD != (R)0, cH != (R)0, B, U, e1, e2);
     }
   }
 }
 
 // add one axis' sums into DB (volume and Hall terms) and the dissipation sum
-template <typename R, bool HALL, bool HOD, int CONV>
-__device__ __forceinline__ void col_combine(const StageArgs<R, SoA<R>> &a, int ax, const ColSums<R> &s,
+template <typename R, bool HALL, bool HOD, int CONV, typename F = SoA<R>>
+__device__ __forceinline__ void col_combine(const StageArgs<R, F> &a, int ax, const ColSums<R> &s,
                                             const V3<R> &Bm, const V3<R> &um, V3<R> &db, V3<R> &hod) {
   if (CONV) {
     const R Ba = cmp(Bm, ax), Ua = cmp(um, ax);
@@ -170,9 +175,10 @@ __device__ __forceinline__ void col_combine(const StageArgs<R, SoA<R>> &a, int a
   }
 }
 
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
-__global__ void __launch_bounds__(kColThreads, CONV ? 256 / kColThreads : IEQ_COL_MIN_BLOCKS * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
+__global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS : IEQ_COL_MIN_BLOCKS) * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
+  const int need = NEED >= 0 ? NEED : a.need;
   constexpr int NZ = col_nodes(CONV);
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -204,8 +210,8 @@ __global__ void __launch_bounds__(kColThreads, CONV ? 256 / kColThreads : IEQ_CO
 #pragma unroll
         for (int ax = 0; ax < 2; ++ax) {
           ColSums<R> s{};
-          col_axis<R, OP, PER, HALL, HOD, CONV>(s, a, ax, ax == 0 ? ix : iy, ax == 0 ? nx : ny, idx,
-                                                ax == 0 ? 1 : nx, Bm[k]);
+          col_axis<R, OP, PER, HALL, HOD, CONV, SoA<R>, NEED>(s, a, ax, ax == 0 ? ix : iy, ax == 0 ? nx : ny, idx,
+                                                             ax == 0 ? 1 : nx, Bm[k]);
           col_combine<R, HALL, HOD, CONV>(a, ax, s, Bm[k], um[k], db[k], hod[k]);
         }
       }
@@ -243,7 +249,7 @@ __global__ void __launch_bounds__(kColThreads, CONV ? 256 / kColThreads : IEQ_CO
           if (o == 0) {
             if (HOD) col_acc<R, false, HOD, 0>(s[k], 2, 0, (R)0, a.Hint[RI], false, true, B, zero, (R)0, (R)0);
           } else {
-            col_acc<R, HALL, HOD, CONV>(s[k], 2, a.need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
+            col_acc<R, HALL, HOD, CONV>(s[k], 2, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
           }
         }
       }
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(kColThreads, CONV ? 256 / kColThreads : IEQ_CO
         if (k < cnt) {
           const long long idx = base + (long long)(iz0 + k) * sz;
           ColSums<R> s{};
-          col_axis<R, OP, PER, HALL, HOD, CONV>(s, a, 2, iz0 + k, nz, idx, sz, Bm[k]);
+          col_axis<R, OP, PER, HALL, HOD, CONV, SoA<R>, NEED>(s, a, 2, iz0 + k, nz, idx, sz, Bm[k]);
           col_combine<R, HALL, HOD, CONV>(a, 2, s, Bm[k], um[k], db[k], hod[k]);
         }
       }

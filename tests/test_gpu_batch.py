@@ -20,8 +20,8 @@ SPECS = [(16, 2, 0.7, 0.5 * (2 / 15) / (0.7 * math.sqrt(2))),
          (17, 4, 0.55, 0.5 * (2 / 16) / (0.55 * math.sqrt(2)))]
 
 
-@pytest.mark.parametrize("persistent", [True, False])
-def test_batched_solves_equal_single_solves(persistent):
+@pytest.mark.parametrize("mode", ["persistent", "stages", "branches"])
+def test_batched_solves_equal_single_solves(mode):
     bt = Batch(SPECS)
     shapes = [(32, 4, 2), (16, 4, 4), (8, 8, 4), (64, 2, 2)]
     for i, s in enumerate(shapes):
@@ -30,7 +30,7 @@ def test_batched_solves_equal_single_solves(persistent):
     b0 = [c.get_vec(f["b"]) for c, f in zip(bt.ctxs, bt.fields)]
     bt.bind()
     steps = 7
-    bt.run(steps, persistent=persistent)
+    bt.run(steps, mode=mode)
     bt.unbind()
     for i, (c, f) in enumerate(zip(bt.ctxs, bt.fields)):
         got = c.get_vec(f["b"])
