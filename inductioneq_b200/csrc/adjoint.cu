@@ -378,6 +378,49 @@ const void *stage_u(ieq_ctx *c, const void *u, void *uw, double *d_time, double 
   return uw;
 }
 
+// work fields of one SSPRK33 step adjoint, allocated once per call of the public entry
+// points (the checkpointed sweep reuses them for every step)
+struct VjpWork {
+  std::vector<void *> f;   // J0, gJr, z, l1, l2, l3, uw
+  double *d_time = nullptr;
+};
+
+ieq_status vjp_work_alloc(ieq_ctx *c, VjpWork &w) {
+  ieq_status st = work_alloc(c, w.f, 7, c->n_pad * sizeof(R4<double>));
+  if (st == IEQ_OK && cudaMalloc(&w.d_time, 2 * sizeof(double)) != cudaSuccess)
+    st = afail(c, IEQ_ERR_CUDA, "adjoint work allocation");
+  return st;
+}
+
+void vjp_work_free(VjpWork &w) {
+  free_all(w.f);
+  if (w.d_time) cudaFree(w.d_time);
+  w.d_time = nullptr;
+}
+
+// lambda <- (d step / d s1)^T lambda for the SSPRK33 step with stage states s1, s2, s3 that
+// started at time t0; enqueued on the context's stream, no allocation, no synchronisation
+ieq_status ssprk33_step_vjp_ws(ieq_ctx *c, const void *s1, const void *s2, const void *s3, double t0, void *lambda,
+                               const void *u, const void *rho, const VjpWork &w) {
+  void *J0 = w.f[0], *gJr = w.f[1], *z = w.f[2], *l1 = w.f[3], *l2 = w.f[4], *l3 = w.f[5], *uw = w.f[6];
+  double *d_time = w.d_time;
+  const double h = c->s.dt;
+  const double t2 = t0 + h, t3 = t0 + 0.5 * h;   // SSPRK33_2a / _3a
+  ieq_status st;
+  // stage 3: lambda3 = 2/3 (lambda + h F'(s3)^T lambda); lambda1 = 1/3 lambda
+  if ((st = vjp(c, s3, lambda, stage_u(c, u, uw, d_time, t3), rho, z, J0, gJr)) != IEQ_OK) return st;
+  lincomb(c, l3, 2.0 / 3.0, lambda, 2.0 / 3.0 * h, z);
+  lincomb(c, l1, 1.0 / 3.0, lambda, 0.0, nullptr);
+  // stage 2: lambda2 = 1/4 (lambda3 + h F'(s2)^T lambda3); lambda1 += 3/4 lambda3
+  if ((st = vjp(c, s2, l3, stage_u(c, u, uw, d_time, t2), rho, z, J0, gJr)) != IEQ_OK) return st;
+  lincomb(c, l2, 0.25, l3, 0.25 * h, z);
+  lincomb(c, l1, 1.0, l1, 0.75, l3);
+  // stage 1: lambda1 += lambda2 + h F'(s1)^T lambda2
+  if ((st = vjp(c, s1, l2, stage_u(c, u, uw, d_time, t0), rho, z, J0, gJr)) != IEQ_OK) return st;
+  lincomb(c, lambda, 1.0, l1, 1.0, l2, h, z);
+  return IEQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -431,30 +474,10 @@ ieq_status ieq_ssprk33_step_vjp(ieq_ctx *c, const void *s1, const void *s2, cons
   ieq_status st = check_adjoint_settings(c);
   if (st != IEQ_OK) return st;
   cudaSetDevice(c->device);
-  std::vector<void *> w;
-  const size_t vb = c->n_pad * sizeof(R4<double>);
-  if ((st = work_alloc(c, w, 7, vb)) != IEQ_OK) return st;
-  void *J0 = w[0], *gJr = w[1], *z = w[2], *l1 = w[3], *l2 = w[4], *l3 = w[5], *uw = w[6];
-  double *d_time = nullptr;
-  cudaMalloc(&d_time, 2 * sizeof(double));
-  const double h = c->s.dt;
-  const double t2 = t0 + h, t3 = t0 + 0.5 * h;   // SSPRK33_2a / _3a
-  // stage 3: lambda3 = 2/3 (lambda + h F'(s3)^T lambda); lambda1 = 1/3 lambda
-  if ((st = vjp(c, s3, lambda, stage_u(c, u, uw, d_time, t3), rho, z, J0, gJr)) != IEQ_OK) goto done;
-  lincomb(c, l3, 2.0 / 3.0, lambda, 2.0 / 3.0 * h, z);
-  lincomb(c, l1, 1.0 / 3.0, lambda, 0.0, nullptr);
-  // stage 2: lambda2 = 1/4 (lambda3 + h F'(s2)^T lambda3); lambda1 += 3/4 lambda3
-  if ((st = vjp(c, s2, l3, stage_u(c, u, uw, d_time, t2), rho, z, J0, gJr)) != IEQ_OK) goto done;
-  lincomb(c, l2, 0.25, l3, 0.25 * h, z);
-  lincomb(c, l1, 1.0, l1, 0.75, l3);
-  // stage 1: lambda1 += lambda2 + h F'(s1)^T lambda2
-  if ((st = vjp(c, s1, l2, stage_u(c, u, uw, d_time, t0), rho, z, J0, gJr)) != IEQ_OK) goto done;
-  lincomb(c, lambda, 1.0, l1, 1.0, l2, h, z);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = afail(c, IEQ_ERR_CUDA, "step vjp");
-done:
-  cudaStreamSynchronize(c->stream);
-  cudaFree(d_time);
-  free_all(w);
+  VjpWork w;
+  if ((st = vjp_work_alloc(c, w)) == IEQ_OK) st = ssprk33_step_vjp_ws(c, s1, s2, s3, t0, lambda, u, rho, w);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "step vjp");
+  vjp_work_free(w);
   return st;
 }
 
@@ -472,11 +495,13 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   const int K = checkpoint_every;
   const int nseg = (num_steps + K - 1) / K;
   std::vector<void *> ck, seg, w;
+  VjpWork vw;
   if ((st = work_alloc(c, ck, nseg, vb)) != IEQ_OK || (st = work_alloc(c, seg, 3 * K, vb)) != IEQ_OK ||
-      (st = work_alloc(c, w, 5, vb)) != IEQ_OK) {
+      (st = work_alloc(c, w, 5, vb)) != IEQ_OK || (st = vjp_work_alloc(c, vw)) != IEQ_OK) {
     free_all(ck);
     free_all(seg);
     free_all(w);
+    vjp_work_free(vw);
     return st;
   }
   void *cur = w[0], *b2 = w[1], *b3 = w[2], *cb = w[3], *uw = w[4];
@@ -517,14 +542,15 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
     for (int n = n0; n < n1 && st == IEQ_OK; ++n)
       st = step(cur, t0s[n], seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2]);
     for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n)
-      st = ieq_ssprk33_step_vjp(c, seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2], t0s[n], lambda, u,
-                                rho);
+      st = ssprk33_step_vjp_ws(c, seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2], t0s[n], lambda, u,
+                               rho, vw);
   }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "adjoint sweep");
   cudaFree(d_time);
   free_all(ck);
   free_all(seg);
   free_all(w);
+  vjp_work_free(vw);
   return st;
 }
 
