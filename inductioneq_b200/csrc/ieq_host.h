@@ -39,7 +39,8 @@ struct Settings {
   bool variable_u = false;
   // kernels of the fused time stepping (IEQ_STAGE_KERNEL): 0 AUTO (the column kernels,
   // measured fastest on B200), 1 COLUMN, 2 NODE (the per-node J-based kernels), 3 BRICK
-  // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN)
+  // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN),
+  // 4 LIST (no fusion: the reference's kernel list of each step on the caller's fields)
   int stage_kernel = 0;
 };
 

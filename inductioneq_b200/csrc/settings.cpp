@@ -124,7 +124,8 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
       else if (val == "COLUMN") s.stage_kernel = 1;
       else if (val == "NODE") s.stage_kernel = 2;
       else if (val == "BRICK") s.stage_kernel = 3;
-      else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE or BRICK"; return false; }
+      else if (val == "LIST") s.stage_kernel = 4;
+      else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE, BRICK or LIST"; return false; }
     } else if (key == "USE_HALL") {
       s.hall = true;
     } else if (key == "USE_PERIODIC") {

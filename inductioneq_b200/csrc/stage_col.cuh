@@ -402,6 +402,27 @@ __global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ 
   }
 }
 
+// SSPRK104_06 (kernel_time_integrator.cl, between stages 5 and 7) on the SoA state:
+// b3 = 0.04 b1 + 0.36 b2; b2 = 0.6 b1 + 0.4 b2; the last block sets time[1] = time[0] + tK
+template <typename R>
+__global__ void k_soa_ssp104_06(long long n, SoA<R> b1, SoA<R> b2, SoA<R> b3, R *time, R tK, unsigned *counter) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) {
+    const V3<R> p = ldf_plain(b1, i), q = ldf_plain(b2, i);
+    stf(b3, i, V3<R>{(R)0.04 * p.x + (R)0.36 * q.x, (R)0.04 * p.y + (R)0.36 * q.y, (R)0.04 * p.z + (R)0.36 * q.z});
+    stf(b2, i, V3<R>{(R)0.60 * p.x + (R)0.40 * q.x, (R)0.60 * p.y + (R)0.40 * q.y, (R)0.60 * p.z + (R)0.40 * q.z});
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(counter, 1u) == gridDim.x - 1) {
+      time[1] = time[0] + tK;
+      __threadfence();
+      *counter = 0u;
+    }
+  }
+}
+
 // launch shape of the column kernels: kColBX x kColBY x kColBZ threads (kColThreads), each
 // `nodes` nodes in z
 inline dim3 col_block() { return dim3(kColBX, kColBY, kColBZ); }

@@ -90,6 +90,7 @@ enum EpilogueMode : int {
   EP_AX_HF = 3,       // out = A*X + h*F               CarpenterKennedy/ToulorgeDesmet "a"
   EP_2N_FUSED = 4,    // t = A*X + h*F; out = t; out2 = Z + Bc*t     ("a" and "b" fused)
   EP_2N_FUSED_FIRST = 5,  // t = h*F; out = t; out2 = Z + Bc*t
+  EP_2R_FUSED = 6,    // t = h*F; out = X + A*t; out2 = out + Bc*t; out3 = t (if set)   (2R "a" + "b")
 };
 
 enum TimePost : int {
@@ -108,7 +109,7 @@ struct StageArgs {
   F E;                  // (column kernel, Hall) J x B as (Jx By - Jy Bx, Jx Bz - Jz Bx, Jy Bz - Jz By)
   F u;
   F X, Y, Z;
-  F out, out2;
+  F out, out2, out3;
   const Tables<R> *tab;
   R *time;
   unsigned *counter;    // last-block ticket for the time post-update
@@ -306,6 +307,7 @@ __device__ __forceinline__ EpIn<R> epilogue_load(const StageArgs<R, F> &a, long 
   switch (a.mode) {
     case EP_X_PLUS_HF:
     case EP_AX_HF:
+    case EP_2R_FUSED:
       e.X = ldf_plain(a.X, idx);
       break;
     case EP_PX_QYHF:
@@ -350,6 +352,14 @@ __device__ __forceinline__ void epilogue_store(const StageArgs<R, F> &a, long lo
       else t = {a.h * db.x, a.h * db.y, a.h * db.z};
       stf(a.out, idx, t);
       stf(a.out2, idx, V3<R>{Y.x + a.Bc * t.x, Y.y + a.Bc * t.y, Y.z + a.Bc * t.z});
+      break;
+    }
+    case EP_2R_FUSED: {
+      const V3<R> t = {a.h * db.x, a.h * db.y, a.h * db.z};
+      const V3<R> o = {X.x + a.A * t.x, X.y + a.A * t.y, X.z + a.A * t.z};
+      stf(a.out, idx, o);
+      stf(a.out2, idx, V3<R>{o.x + a.Bc * t.x, o.y + a.Bc * t.y, o.z + a.Bc * t.z});
+      if (a.out3.p) stf(a.out3, idx, t);
       break;
     }
   }

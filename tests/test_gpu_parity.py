@@ -245,19 +245,45 @@ def test_fused_time_steps_are_bitwise_reproducible(name):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
-@pytest.mark.parametrize("name", ["rot3d_2c_ck2n54", "wave_6c_hall_hod_ck2n54"])
+@pytest.mark.parametrize("name", ["rot3d_2c_ck2n54", "wave_6c_hall_hod_ck2n54", "rot3d_4e_split_kcl",
+                                  "confined_6e_hall_fo_cfr", "hallper_4c_ssprk104_varu", "alfven_2e_adaptive_td"])
 def test_fused_odd_and_even_step_counts(name):
-    # the fused 5-stage 2N step ping-pongs b1; odd counts copy the result back
+    # the fused 2N and 2R steps ping-pong b1 / b2; odd counts copy the result back from the
+    # other buffers of the pairs
     z, _ = _golden()
     c = STEP_CASES[name]
     ctx = maps_for(c).context()
     o = oracle_for(c)
+    nf = NUM_FIELDS[c["integrator"]]
     for n in (1, 2, 3):
         host, dev = _fields(ctx, o, z, name)
-        time_loop(o, c["integrator"], c.get("hall", False), False, n, host[0], host[1], None, host[3],
-                  host[4], host[5], host[6])
+        time_loop(o, c["integrator"], c.get("hall", False), c.get("variable_u", False), n, host[0], host[1],
+                  host[2] if nf == 3 else None, host[3], host[4], host[5], host[6])
         ctx.time_steps(*dev, n)
-        assert rel_err(ctx.get_vec(dev[0]), host[0]) <= TOL64, n
+        assert rel_err(ctx.get_vec(dev[0]), host[0]) <= tol(c), n
+        assert rel_err(ctx.get_vec(dev[1]), host[1]) <= tol(c), n
+        if nf == 3:
+            assert rel_err(ctx.get_vec(dev[2]), host[2]) <= tol(c), n
+        np.testing.assert_allclose(ctx.get_scalar(dev[6], n=2), host[6], rtol=1e-15)
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_fused_steps_equal_reference_kernel_lists(name):
+    # IEQ_STAGE_KERNEL=LIST runs each step as the reference's kernel list on the caller's
+    # fields; the fused path must agree with it
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    o = oracle_for(c)
+    nf = NUM_FIELDS[c["integrator"]]
+    out = []
+    for kernel in ("AUTO", "LIST"):
+        ctx = maps_for(dict(c, stage_kernel=kernel)).context()
+        _, dev = _fields(ctx, o, z, name)
+        ctx.time_steps(*dev, 3)
+        out.append([ctx.get_vec(dev[i]) for i in range(nf)] + [ctx.get_scalar(dev[6], n=2)])
+    for i in range(nf):
+        assert rel_err(out[0][i], out[1][i]) <= 10 * tol(c), i
+    np.testing.assert_allclose(out[0][-1], out[1][-1], rtol=1e-15)
 
 
 @pytest.mark.parametrize("name", ["rot_gauss_4c_ssprk33", "rot3d_2c_ck2n54"])
