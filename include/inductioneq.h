@@ -106,6 +106,19 @@ ieq_status ieq_run_kernels_host(ieq_ctx *ctx, const char *const *names, int n_na
 ieq_status ieq_time_steps(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
                           void *rho, void *time, int num_steps);
 
+/* ieq_time_steps with the per-step diagnostics of the reference's save_integrals_over_time
+ * loop (compute_numerical_solution.m:153-193): before every step the mass-weighted energy
+ * norm2(b), the divergence norm sqrt(norm2_S(calc_div(b))) and the L2 error
+ * sqrt(norm2_diff(b, analytical_b(time[0]))) are evaluated on the device in one pass and
+ * collected into a device series (inside the step graph when there is no cleaning).  With
+ * clean_max_iterations > 0, B is cleaned after every step (ieq_clean_div with that cap and
+ * clean_threshold), as the reference does when divergence cleaning is on.  energy,
+ * divergence_norm, l2_error: host arrays of num_steps entries, or NULL.  Synchronises. */
+ieq_status ieq_time_steps_integrals(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
+                                    void *rho, void *time, int num_steps, int clean_max_iterations,
+                                    double clean_threshold, double *energy, double *divergence_norm,
+                                    double *l2_error);
+
 /* Divergence cleaning, matlab/+induction_eq/clean_div.m:36-79, device resident: CG on
  * (-Laplace) phi = div B over the interior, stopping when the unweighted squared
  * residual <= absolute_error_threshold^2 or after max_iterations, then B is projected.

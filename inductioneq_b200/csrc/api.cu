@@ -10,6 +10,7 @@
 #include "ieq_host.h"
 #include "misc_kernels.cuh"
 #include "stage_brick.cuh"
+#include "diag.cuh"
 
 namespace ieq {
 void free_brick_maps(ieq_ctx *c);   // api_fused.inc

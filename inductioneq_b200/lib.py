@@ -76,6 +76,8 @@ def load() -> ctypes.CDLL:
                                          ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
                                          ctypes.POINTER(sz), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.ieq_time_steps.argtypes = [vp] * 8 + [ctypes.c_int]
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.ieq_time_steps_integrals.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
     lib.ieq_clean_div.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     for f in ("ieq_norm2_value", "ieq_norm2_S_value"):
@@ -221,6 +223,20 @@ class Context:
     def time_steps(self, b, b2, b3, curlB_rho, u, rho, time, num_steps: int) -> None:
         self._check(self.lib.ieq_time_steps(self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u),
                                             _ptr(rho), _ptr(time), int(num_steps)))
+
+    def time_steps_integrals(self, b, b2, b3, curlB_rho, u, rho, time, num_steps: int, clean_max_iterations: int = 0,
+                             clean_threshold: float = 0.0) -> dict:
+        """time_steps with the per-step series of save_integrals_over_time: energy, divergence
+        norm and L2 error of b before every step (numpy arrays of num_steps entries); with
+        clean_max_iterations > 0 B is cleaned after every step."""
+        n = int(num_steps)
+        e, d, l = (np.zeros(max(n, 1)) for _ in range(3))
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.ieq_time_steps_integrals(
+            self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u), _ptr(rho), _ptr(time), n,
+            int(clean_max_iterations), float(clean_threshold), e.ctypes.data_as(dp), d.ctypes.data_as(dp),
+            l.ctypes.data_as(dp)))
+        return {"energy": e[:n], "divergence_norm": d[:n], "l2_error": l[:n]}
 
     def clean_div(self, b, max_iterations: int, absolute_error_threshold: float, check: bool = True):
         it = ctypes.c_int(0)

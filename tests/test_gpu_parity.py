@@ -15,7 +15,7 @@ import pytest
 
 from oracle.hostloops import clean_div, norms, time_loop
 from oracle.sequencing import NUM_FIELDS, rk_step
-from tests.golden.cases import CG_CASES, NOISE_SEED, STEP_CASES
+from tests.golden.cases import CG_CASES, NOISE_AMPLITUDE, NOISE_SEED, STEP_CASES
 from tests.helpers import maps_for, oracle_for, rel_err
 
 pytestmark = pytest.mark.gpu
@@ -378,3 +378,73 @@ def test_operators_match_oracle():
     outh = o.vec()
     o.run("calc_grad", n, s, outh)
     assert rel_err(ctx.get_vec(outd), outh) <= 1e-12
+
+
+def _oracle_series(o, c, host, steps, clean=None):
+    """energy, ||div B|| and L2 error before every step, then the step (and the cleaning),
+    as compute_numerical_solution.m:121-193 runs them"""
+    nf = NUM_FIELDS[c["integrator"]]
+    out = {"energy": [], "divergence_norm": [], "l2_error": []}
+    for _ in range(steps):
+        ana = o.vec()
+        o.run("analytical_b", o.cfg.nodes, ana, host[6].copy())
+        r = norms(o, host[0].copy(), ana, o.scalar())
+        out["energy"].append(r["energy"])
+        out["divergence_norm"].append(r["divergence_norm"])
+        out["l2_error"].append(r["abs_err"])
+        time_loop(o, c["integrator"], c.get("hall", False), c.get("variable_u", False), 1, host[0], host[1],
+                  host[2] if nf == 3 else None, host[3], host[4], host[5], host[6])
+        if clean:
+            clean_div(o, host[0], clean[0], clean[1], c.get("bnodes", 1))
+    return {k: np.array(v) for k, v in out.items()}
+
+
+def _series_close(got, ref, c, o):
+    rt = 1e-5 if c.get("real") == "float" else 1e-11
+    floor = (1e-6 if c.get("real") == "float" else 1e-13) * float(np.max(ref["energy"])) ** 0.5 / min(o.d)
+    # the error of a field equal to the exact one and ||div B|| of a nearly divergence-free
+    # field are cancellations: their absolute errors are set by the rounding of B
+    np.testing.assert_allclose(got["energy"], ref["energy"], rtol=rt, atol=1e-300)
+    np.testing.assert_allclose(got["l2_error"], ref["l2_error"], rtol=rt, atol=floor * min(o.d))
+    np.testing.assert_allclose(got["divergence_norm"], ref["divergence_norm"], rtol=rt, atol=floor)
+
+
+@pytest.mark.parametrize("name", ["rot_gauss_4c_ssprk33", "wave_6c_hall_hod_ck2n54", "rot3d_4e_split_kcl",
+                                  "hallper_4c_ssprk104_varu", "rot_gauss_4c_ssprk33_f32"])
+def test_time_steps_integrals_match_oracle(name):
+    # the per-step series of save_integrals_over_time, collected inside the step graph
+    z, _ = _golden()
+    c = STEP_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    steps = 3
+    host, dev = _fields(ctx, o, z, name)
+    got = ctx.time_steps_integrals(*dev, steps)
+    ref = _oracle_series(o, c, host, steps)
+    _series_close(got, ref, c, o)
+    # the diagnostics do not change the stepping
+    _, dev2 = _fields(ctx, o, z, name)
+    ctx.time_steps(*dev2, steps)
+    np.testing.assert_array_equal(ctx.get_vec(dev[0]), ctx.get_vec(dev2[0]))
+    np.testing.assert_array_equal(ctx.get_scalar(dev[6], n=2), ctx.get_scalar(dev2[6], n=2))
+
+
+def test_time_steps_integrals_with_cleaning_match_oracle():
+    # divergence cleaning after every step (compute_numerical_solution.m:129-147)
+    c = dict(order=4, testcase="confined_domain", nodes=(14, 15, 16), lo=0.0, hi=1.0, hall=True,
+             integrator="CarpenterKennedy2N54", dt=2e-4, laplace="WIDE_STENCIL_DIRICHLET", bnodes=1)
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    b = ctx.vec()
+    ctx.kernel("init_b", b)
+    bh = ctx.get_vec(b).astype(np.float64)
+    bh[: ctx.n, :3] += NOISE_AMPLITUDE * np.random.default_rng(NOISE_SEED).random((ctx.n, 3))
+    zero = np.zeros_like(bh)
+    host = [bh.copy(), zero.copy(), zero.copy(), zero.copy(), zero.copy(), np.ones(o.N), np.zeros(2)]
+    dev = [ctx.vec(bh), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+           ctx.scalar(np.zeros(2), n=2)]
+    steps, clean = 2, (60, 1e-9)
+    got = ctx.time_steps_integrals(*dev, steps, clean_max_iterations=clean[0], clean_threshold=clean[1])
+    ref = _oracle_series(o, c, host, steps, clean)
+    _series_close(got, ref, c, o)
+    assert rel_err(ctx.get_vec(dev[0]), host[0]) <= 1e-10
