@@ -286,6 +286,47 @@ def form_batched(dev, steps=200):
             "seed": 2026}
 
 
+def sharded_batch(rk, dev, steps=200, reps=3):
+    """The 32-solve batch split between the ranks (inductioneq_b200.ranks.partition on
+    nodes x stages; no communication in the data path): every rank runs its solves as one
+    graph of per-solve branches; value = all solves' DOF-updates / max-over-ranks time
+    (strong scaling: the batch is fixed)."""
+    import torch
+
+    from inductioneq_b200 import ranks as R
+    from inductioneq_b200.batch import Batch, rotation_batch
+    specs = rotation_batch(32, seed=2026)
+    parts = R.partition([n ** 3 for (n, _, _, _) in specs], rk.world)
+    mine = [specs[i] for i in parts[rk.rank]]
+    total_nodes = sum(n ** 3 for (n, _, _, _) in specs)
+    t = 0.0
+    if mine:
+        bt = Batch(mine, device=dev)
+        stream = torch.cuda.ExternalStream(bt.stream, device=dev)
+        bt.init()
+        bt.bind()
+        bt.run(steps, mode="branches")   # capture + warm
+        times = []
+        for _ in range(reps):
+            bt.init()
+            bt.bind()
+            R.barrier(rk)
+            times.append(events_time(stream, lambda: bt.run(steps, mode="branches")))
+        bt.unbind()
+        bt.close()
+        t = statistics.median(times)
+    else:
+        for _ in range(reps):
+            R.barrier(rk)
+    t_max = R.max_over_ranks(rk, t, device="cuda")
+    return {"metric": METRIC + " (batched form, 32 rotation solves split between the GPUs)",
+            "value": 3 * total_nodes * 3 * steps / t_max, "unit": "DOF/s", "n_gpus": rk.world,
+            "ms_per_run": t_max * 1e3, "higher_is_better": True, "scaling": "strong", "dtype": "f64",
+            "data": "synthetic (seeded rotation batch, seed 2026)",
+            "config": {"workload": "32 rotation solves, N ~ U{16..96}, orders 2/4/6, 200 SSPRK33 steps",
+                       "solves_per_rank": [len(p) for p in parts], "mode": "branches"}}
+
+
 def form_precision(dev, n=128, steps=20):
     """Confined-domain Hall case on 128^3: FP32 state with FP64 CG cleaning to ||r||_2 < 1e-10,
     then CK2N54 steps; compared with the FP64 run."""
@@ -434,10 +475,12 @@ def main() -> None:
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 / batched / precision lines")
     ap.add_argument("--stage-kernel", choices=("AUTO", "COLUMN", "BRICK"), default="AUTO",
                     help="kernels of the fused stages (IEQ_STAGE_KERNEL)")
+    ap.add_argument("--sharded-batch", action="store_true",
+                    help="only the batched form, its 32 solves split between the ranks")
     a = ap.parse_args()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from inductioneq_b200 import ranks as R
+    rk = R.Ranks.from_env()
+    world, rank, local_rank = rk.world, rk.rank, rk.local_rank
 
     if a.impl == "reference":
         if rank != 0:
@@ -458,12 +501,16 @@ def main() -> None:
 
     import numpy as np
     import torch
-    import torch.distributed as dist
 
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    R.init(rk, "nccl", timeout_s=120.0)
     dev = local_rank
     torch.cuda.set_device(dev)
+    if a.sharded_batch:
+        line = sharded_batch(rk, dev)
+        if rank == 0:
+            print(json.dumps(line))
+        R.finish(rk)
+        return
     m = maps()
     m.I_Tech["stage_kernel"] = a.stage_kernel
     ctx = m.context(device=dev)
@@ -479,8 +526,7 @@ def main() -> None:
     flush = ctx.alloc(256 << 20)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        R.barrier(rk)
 
     def solve():
         b.upload(b0)
@@ -523,11 +569,7 @@ def main() -> None:
     clk = clocks.stop()
     step_ms = [s_.elapsed_time(e_) for s_, e_ in ev]
     t_total = sum(step_ms) * 1e-3
-    t_max = t_total
-    if world > 1:
-        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max = R.max_over_ranks(rk, t_total, device="cuda")
     dof = 3 * nn * STAGES * NUM_STEPS_FULL * K * world
     value = dof / t_max
     stage_ms = [ms for rec in prof for (nm, ms) in rec if nm.startswith("stage")]
@@ -556,11 +598,7 @@ def main() -> None:
         ctx._check(ctx.lib.ieq_download(ctx.h, h_out.data_ptr(), b.ptr, h_out.numel() * 8))
         eev[k][1].record(stream)
     ctx.synchronize()
-    e2e_t = sum(s_.elapsed_time(e_) for s_, e_ in eev) * 1e-3
-    if world > 1:
-        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t = R.max_over_ranks(rk, sum(s_.elapsed_time(e_) for s_, e_ in eev) * 1e-3, device="cuda")
     e2e_value = 3 * nn * STAGES * NUM_STEPS_FULL * Ke * world / e2e_t
 
     # ---------------- roofline of the dominant kernel (fused stage kernel)
@@ -633,8 +671,7 @@ def main() -> None:
     if rank == 0:
         print(json.dumps(out))
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.finish(rk)
 
 
 if __name__ == "__main__":
