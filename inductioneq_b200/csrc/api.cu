@@ -220,15 +220,15 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
 }
 
 template <typename R>
-void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv) {
+void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, bool hodp = false) {
   const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
   switch (c->op_id) {
-    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, c->stream); break;
-    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, c->stream); break;
-    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, c->stream); break;
-    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, c->stream); break;
-    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, c->stream); break;
-    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, c->stream); break;
+    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, c->stream); break;
   }
 }
 
@@ -237,17 +237,28 @@ CurlArgs<R, F> curl_args(ieq_ctx *c, F b, const R *rho, F out);
 
 // E = J x B with J = curl(b)/rho, and J on the faces of a non-periodic box
 template <typename R>
-void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jface) {
+void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jface, SoA<R> hout = SoA<R>{}) {
   CurlArgs<R, SoA<R>> a = curl_args<R, SoA<R>>(c, b, rho, E);
   a.jface = jface;
+  a.hout = hout;
+  const bool hod = hout.p != nullptr;
+  if (hod) {
+    // the interior dissipation row, as stage_base forms it
+    const SbpOperator &op = c->op;
+    const int RI = op.order / 2, WH = op.w_hod;
+    const R sgn = ((op.order / 2 + 1) % 2) ? (R)-1 : (R)1;
+    for (int s = -WH + 1; s <= 0; ++s)
+      for (int i = 0; i < WH; ++i)
+        a.Hint[s + i + RI] += (((R)op.minv[op.nb] * (R)op.DHO.at(op.nb, s + WH - 1)) * (R)op.DHO.at(op.nb, i)) * sgn;
+  }
   const bool per = c->s.periodic;
   switch (c->op_id) {
-    case 0: launch_curl_e<R, 0>(a, per, c->stream); break;
-    case 1: launch_curl_e<R, 1>(a, per, c->stream); break;
-    case 2: launch_curl_e<R, 2>(a, per, c->stream); break;
-    case 3: launch_curl_e<R, 3>(a, per, c->stream); break;
-    case 4: launch_curl_e<R, 4>(a, per, c->stream); break;
-    case 5: launch_curl_e<R, 5>(a, per, c->stream); break;
+    case 0: launch_curl_e<R, 0>(a, per, hod, c->stream); break;
+    case 1: launch_curl_e<R, 1>(a, per, hod, c->stream); break;
+    case 2: launch_curl_e<R, 2>(a, per, hod, c->stream); break;
+    case 3: launch_curl_e<R, 3>(a, per, hod, c->stream); break;
+    case 4: launch_curl_e<R, 4>(a, per, hod, c->stream); break;
+    case 5: launch_curl_e<R, 5>(a, per, hod, c->stream); break;
   }
 }
 

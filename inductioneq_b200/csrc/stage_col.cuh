@@ -175,9 +175,12 @@ __device__ __forceinline__ void col_combine(const StageArgs<R, F> &a, int ax, co
   }
 }
 
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
+// HODP: the dissipation sum comes precomputed (a.Hpre, written by k_curl_e_hod in the
+// same order of operations) instead of being gathered here
+template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, int NEED = -1, bool HODP = false>
 __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS : IEQ_COL_MIN_BLOCKS) * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
+  constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
   const int need = NEED >= 0 ? NEED : a.need;
   constexpr int NZ = col_nodes(CONV);
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
@@ -274,10 +277,11 @@ __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS :
         const long long idx = base + (long long)(iz0 + k) * sz;
         V3<R> d = db[k];
         if (!PER) stage_sat<R, SoA<R>, HALL>(a, ii, nn, idx, Bm[k], um[k], CONV, d);
-        if (HOD) {
-          d.x += a.hod_factor * hod[k].x;
-          d.y += a.hod_factor * hod[k].y;
-          d.z += a.hod_factor * hod[k].z;
+        if (HOD_) {
+          const V3<R> hv = HODP ? ldf(a.Hpre, idx) : hod[k];
+          d.x += a.hod_factor * hv.x;
+          d.y += a.hod_factor * hv.y;
+          d.z += a.hod_factor * hv.z;
         }
         stage_epilogue<R, SoA<R>>(a, idx, d);
       }
@@ -402,6 +406,87 @@ __global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ 
   }
 }
 
+// J = curl(B)/rho, E = J x B and, for the dissipation of the next stage kernel, the sum over
+// the axes of the dissipation rows of B (one node per thread).  Every axis loads all three
+// components of B at its stencil points once: the two orthogonal components feed the curl,
+// all three the dissipation rows, in the order k_stage_col gathers them (so the stored sum
+// equals the one the stage kernel would form).
+// register cap of k_curl_e_hod (measured: <= 64 registers, 8 CTAs of 128 threads per SM,
+// is 4-23 % faster than the uncapped 60-register build at 64^3 .. 128^3)
+#ifndef IEQ_CURL_MIN_BLOCKS
+#define IEQ_CURL_MIN_BLOCKS 8
+#endif
+template <typename R, int OP, bool PER>
+__global__ void __launch_bounds__(kColThreads, IEQ_CURL_MIN_BLOCKS * 128 / kColThreads)
+    k_curl_e_hod(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
+  constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= nx || iy >= ny || iz >= nz) return;
+  const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {nx, ny, nz};
+  const long long st[3] = {1, nx, (long long)nx * ny};
+  const V3<R> Bm = ldf(a.b, idx);
+  R g[3][3];
+  V3<R> hod = {0, 0, 0};
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+    R v1 = 0, v2 = 0;
+    V3<R> ho = {0, 0, 0};
+    const int i = ii[ax], n = nn[ax];
+    const int row = PER ? NB : sbp_row(i, n, NB);
+    if (row == NB) {
+      const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) {
+        const R cH = a.Hint[o + RI];
+        if (o == 0) {
+          ho.x += cH * Bm.x; ho.y += cH * Bm.y; ho.z += cH * Bm.z;
+          continue;
+        }
+        const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
+        const V3<R> B = ldf(a.b, j);
+        const R c = a.Dint[o + RI];
+        v1 += c * cmp(B, c1);
+        v2 += c * cmp(B, c2);
+        ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
+      }
+    } else {
+      for (int o = -RB; o <= RB; ++o) {
+        const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+        const R cH = (o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+        if (cD == (R)0 && cH == (R)0) continue;
+        const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
+        const V3<R> B = ldf(a.b, j);
+        if (cD != (R)0) {
+          v1 += cD * cmp(B, c1);
+          v2 += cD * cmp(B, c2);
+        }
+        if (cH != (R)0) {
+          ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
+        }
+      }
+    }
+    g[ax][c1] = v1 * a.inv_d[ax];
+    g[ax][c2] = v2 * a.inv_d[ax];
+    hod.x += ho.x; hod.y += ho.y; hod.z += ho.z;
+  }
+  V3<R> J = {g[1][2] - g[2][1], g[2][0] - g[0][2], g[0][1] - g[1][0]};
+  if (a.rho) {
+    const R r = (R)1 / a.rho[idx];
+    J = {J.x * r, J.y * r, J.z * r};
+  }
+  stf(a.out, idx, V3<R>{J.x * Bm.y - J.y * Bm.x, J.x * Bm.z - J.z * Bm.x, J.y * Bm.z - J.z * Bm.y});
+  stf(a.hout, idx, hod);
+  if (!PER && (ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1))
+    stf(a.jface, idx, J);
+}
+
 // SSPRK104_06 (kernel_time_integrator.cl, between stages 5 and 7) on the SoA state:
 // b3 = 0.04 b1 + 0.36 b2; b2 = 0.6 b1 + 0.4 b2; the last block sets time[1] = time[0] + tK
 template <typename R>
@@ -433,8 +518,9 @@ inline dim3 col_grid(int nx, int ny, int nz, int nodes) {
 }
 
 template <typename R, int OP>
-void launch_stage_col(const StageArgs<R, SoA<R>> &a, bool per, bool hall, bool hod, int conv, cudaStream_t s);
+void launch_stage_col(const StageArgs<R, SoA<R>> &a, bool per, bool hall, bool hod, int conv, bool hodp,
+                      cudaStream_t s);
 template <typename R, int OP>
-void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, cudaStream_t s);
+void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, bool hod, cudaStream_t s);
 
 }  // namespace ieq

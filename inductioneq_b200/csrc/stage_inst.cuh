@@ -63,10 +63,14 @@ void launch_curl<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a
 
 // the column kernels of the fused path (no first-order / adaptive dissipation)
 template <bool P, bool H>
-static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, dim3 g, dim3 b, cudaStream_t s) {
+static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, dim3 g, dim3 b,
+                          cudaStream_t s) {
   // (a flux-form mask compiled in for the default forms measured 3-10 % slower for orders
   // 4 and 6 on B200: the mask stays a run-time value)
-  if (hod) {
+  if (hod && hodp) {
+    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1, -1, true><<<g, b, 0, s>>>(a);
+    else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0, -1, true><<<g, b, 0, s>>>(a);
+  } else if (hod) {
     if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1><<<g, b, 0, s>>>(a);
     else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0><<<g, b, 0, s>>>(a);
   } else {
@@ -77,20 +81,29 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
 
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
-                                     cudaStream_t s) {
+                                     bool hodp, cudaStream_t s) {
   const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block();
+  // the precomputed dissipation sum comes with the Hall curl kernel only
+  hodp = hodp && hall && hod;
   if (per) {
-    if (hall) launch_col_ph<true, true>(a, hod, conv, g, b, s);
-    else launch_col_ph<true, false>(a, hod, conv, g, b, s);
+    if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, g, b, s);
+    else launch_col_ph<true, false>(a, hod, conv, false, g, b, s);
   } else {
-    if (hall) launch_col_ph<false, true>(a, hod, conv, g, b, s);
-    else launch_col_ph<false, false>(a, hod, conv, g, b, s);
+    if (hall) launch_col_ph<false, true>(a, hod, conv, hodp, g, b, s);
+    else launch_col_ph<false, false>(a, hod, conv, false, g, b, s);
   }
 }
 
 template <>
-void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, cudaStream_t s) {
-  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, kCurlNodes), b = col_block();
+void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hod, cudaStream_t s) {
+  const dim3 b = col_block();
+  if (hod) {
+    const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, 1);
+    if (per) k_curl_e_hod<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
+    else k_curl_e_hod<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
+    return;
+  }
+  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
   if (per) k_curl_e<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
   else k_curl_e<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
 }

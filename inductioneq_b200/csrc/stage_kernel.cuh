@@ -107,6 +107,7 @@ struct StageArgs {
   F bk;                 // field the derivative is taken of
   F J;                  // curl(B)/rho (Hall; the column kernel reads it on faces only)
   F E;                  // (column kernel, Hall) J x B as (Jx By - Jy Bx, Jx Bz - Jz Bx, Jy Bz - Jz By)
+  F Hpre;               // (column kernel) the dissipation sum of bk, precomputed by k_curl_e_hod
   F u;
   F X, Y, Z;
   F out, out2, out3;
@@ -502,6 +503,8 @@ struct CurlArgs {
   const R *rho;       // nullptr: plain curl (kernel_operator.cl:158 calc_curl)
   F out;
   F jface;      // (k_curl_e) J on the faces of a non-periodic box
+  F hout;       // (k_curl_e_hod) the dissipation sum of b (sum over the axes of the H rows)
+  R Hint[7];    // (k_curl_e_hod) interior dissipation row, offsets -RI..RI
   const Tables<R> *tab;
   R dR[3];
   R inv_d[3];   // (REAL)(1.0/DX) ...
