@@ -40,10 +40,13 @@ WORKLOAD = ("hall_circular_wave 64^3 periodic [0,2pi]^3, FP64, 6th-order classic
 METRIC = "DOF-updates/s per RK stage"
 L2_NOTE = ("L2 flushed between timed solves (256 MiB memset on the solver stream, outside the events); "
            "within a solve the 64^3 fields stay L2 resident, as in production")
-# algorithmic bytes per node of one fused CK2N54 Hall stage kernel with J = curl(B)/rho
-# materialised by its own kernel: read b1, J, b2 (3 x 24 B), write b2, b1' (2 x 24 B)
-STAGE_BYTES_PER_NODE = 5 * 24
-CURL_BYTES_PER_NODE = 24 + 8 + 24
+# algorithmic bytes per node of one CK2N54 Hall stage, the compulsory traffic of the
+# stage with curl(B)/rho not materialised: read b1, b2, u (3 x 24 B) and rho (8 B), write
+# b1, b2 (2 x 24 B).  The stage kernel is charged with all of it (the curl kernel, whose
+# own traffic -- read b, rho; write E, H: 80 B -- is extra, is reported beside it)
+STAGE_BYTES_PER_NODE = 3 * 24 + 8 + 2 * 24
+CURL_BYTES_PER_NODE = 24 + 8 + 2 * 24
+FP32_STAGE_BYTES_PER_NODE = 3 * 12 + 4 + 2 * 12
 
 
 def maps(n=N_GRID):
@@ -208,8 +211,9 @@ def form_fp32(dev, b_ref64):
     value = 3 * N_GRID ** 3 * STAGES * NUM_STEPS_FULL * reps / tt
     return {"value": value, "unit": "DOF/s", "ms_per_solve": tt / reps * 1e3, "l2_rel_err_vs_exact": res["rel_err"],
             "max_rel_diff_vs_fp64": vs64, "stage_kernel_ms": stage,
-            "roofline": {"bound": "hbm", "achieved": 60 * N_GRID ** 3 / (stage * 1e-3) / 1e9, "unit": "GB/s",
-                         "algorithmic_bytes_per_node": 60},
+            "roofline": {"bound": "hbm", "achieved": FP32_STAGE_BYTES_PER_NODE * N_GRID ** 3 / (stage * 1e-3) / 1e9,
+                         "unit": "GB/s",
+                         "algorithmic_bytes_per_node": FP32_STAGE_BYTES_PER_NODE},
             "note": "same workload, FP32 state and stencils"}
 
 
@@ -618,8 +622,11 @@ def main() -> None:
                 "peak_source": peak_src, "traffic": None,
                 "algorithmic_bytes_per_node": STAGE_BYTES_PER_NODE, "nodes_per_launch": nn,
                 "avg_launch_ms": stage_avg * 1e3, "curl_kernel_avg_ms": curl_avg * 1e3,
+                "curl_kernel_bytes_per_node": CURL_BYTES_PER_NODE,
+                "stage_pair_frac": STAGE_BYTES_PER_NODE * nn / (stage_avg + curl_avg) / 1e9 / peak,
                 "note": "CUDA events around a graph of 20 back-to-back launches of each kernel of one step "
-                        "(L2 warm, as inside a solve)"}
+                        "(L2 warm, as inside a solve); stage_pair_frac charges the stage's compulsory bytes "
+                        "to the curl and stage kernels together"}
     # DRAM bytes (read + write) of one launch of the stage kernel, from the ncu capture
     # summarised in profiles/ ("traffic_bytes_per_launch: N" line of the kernel's summary)
     kname = "k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col"
@@ -629,8 +636,8 @@ def main() -> None:
             for line in f:
                 if line.startswith("traffic_bytes_per_launch:"):
                     roofline["traffic"] = int(line.split(":", 1)[1].strip())
-                    roofline["traffic_note"] = ("ncu capture with caches flushed before the launch: the inputs b1 and "
-                                                "E come from DRAM, the writes stay in L2")
+                    roofline["traffic_note"] = ("ncu capture with caches flushed before the launch: the inputs "
+                                                "come from DRAM, the writes stay in L2")
 
     out = {
         "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
