@@ -222,13 +222,14 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
 template <typename R>
 void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, bool hodp = false) {
   const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
+  const bool foad = diss_kind(c->s) == DISS_FO_OR_AD;
   switch (c->op_id) {
-    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, c->stream); break;
-    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, c->stream); break;
-    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, hodp, c->stream); break;
-    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, c->stream); break;
-    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, c->stream); break;
-    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, c->stream); break;
+    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
   }
 }
 

@@ -177,7 +177,9 @@ __device__ __forceinline__ void col_combine(const StageArgs<R, F> &a, int ax, co
 
 // HODP: the dissipation sum comes precomputed (a.Hpre, written by k_curl_e_hod in the
 // same order of operations) instead of being gathered here
-template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, int NEED = -1, bool HODP = false>
+// FOAD: first-order or adaptive dissipation (fo_ad_dissipation, after the SAT terms)
+template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, int NEED = -1, bool HODP = false,
+          bool FOAD = false>
 __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS : IEQ_COL_MIN_BLOCKS) * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
@@ -282,6 +284,11 @@ __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS :
           d.x += a.hod_factor * hv.x;
           d.y += a.hod_factor * hv.y;
           d.z += a.hod_factor * hv.z;
+        }
+        if (FOAD) {
+          const long long st[3] = {1, nx, sz};
+          const V3<R> ds = fo_ad_dissipation<R, SoA<R>, OP, PER>(a, ii, nn, st, idx, Bm[k], um[k]);
+          d.x += ds.x; d.y += ds.y; d.z += ds.z;
         }
         stage_epilogue<R, SoA<R>>(a, idx, d);
       }
@@ -519,7 +526,7 @@ inline dim3 col_grid(int nx, int ny, int nz, int nodes) {
 
 template <typename R, int OP>
 void launch_stage_col(const StageArgs<R, SoA<R>> &a, bool per, bool hall, bool hod, int conv, bool hodp,
-                      cudaStream_t s);
+                      bool foad, cudaStream_t s);
 template <typename R, int OP>
 void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, bool hod, cudaStream_t s);
 

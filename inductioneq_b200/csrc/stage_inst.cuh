@@ -63,11 +63,14 @@ void launch_curl<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a
 
 // the column kernels of the fused path (no first-order / adaptive dissipation)
 template <bool P, bool H>
-static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, dim3 g, dim3 b,
-                          cudaStream_t s) {
+static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
+                          dim3 b, cudaStream_t s) {
   // (a flux-form mask compiled in for the default forms measured 3-10 % slower for orders
   // 4 and 6 on B200: the mask stays a run-time value)
-  if (hod && hodp) {
+  if (foad) {
+    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1, -1, false, true><<<g, b, 0, s>>>(a);
+    else k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0, -1, false, true><<<g, b, 0, s>>>(a);
+  } else if (hod && hodp) {
     if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1, -1, true><<<g, b, 0, s>>>(a);
     else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0, -1, true><<<g, b, 0, s>>>(a);
   } else if (hod) {
@@ -81,16 +84,16 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
 
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
-                                     bool hodp, cudaStream_t s) {
+                                     bool hodp, bool foad, cudaStream_t s) {
   const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block();
   // the precomputed dissipation sum comes with the Hall curl kernel only
-  hodp = hodp && hall && hod;
+  hodp = hodp && hall && hod && !foad;
   if (per) {
-    if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, g, b, s);
-    else launch_col_ph<true, false>(a, hod, conv, false, g, b, s);
+    if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, foad, g, b, s);
+    else launch_col_ph<true, false>(a, hod, conv, false, foad, g, b, s);
   } else {
-    if (hall) launch_col_ph<false, true>(a, hod, conv, hodp, g, b, s);
-    else launch_col_ph<false, false>(a, hod, conv, false, g, b, s);
+    if (hall) launch_col_ph<false, true>(a, hod, conv, hodp, foad, g, b, s);
+    else launch_col_ph<false, false>(a, hod, conv, false, foad, g, b, s);
   }
 }
 

@@ -210,8 +210,9 @@ __device__ V3<R> fo_ad_dissipation(const StageArgs<R, F> &a, const int ii[3], co
     V3<R> tmp = {0, 0, 0};
     for (int c = 0; c < SW; ++c) {
       const int o = c - C0;
-      const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
       const R cd = fabs(a.tab->D[row][c]);
+      if (cd == (R)0) continue;   // a zero coefficient adds a zero term: skip its loads
+      const long long j = idx + (long long)(nbr<PER>(ii[ax], o, nn[ax]) - ii[ax]) * st[ax];
       const V3<R> Bk = ldf(a.bk, j);
       const V3<R> uk = ldf(a.u, j);
       V3<R> sg = {fmax(fabs(uk.x), fabs(um.x)), fmax(fabs(uk.y), fabs(um.y)), fmax(fabs(uk.z), fabs(um.z))};
