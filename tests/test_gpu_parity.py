@@ -448,3 +448,32 @@ def test_time_steps_integrals_with_cleaning_match_oracle():
     ref = _oracle_series(o, c, host, steps, clean)
     _series_close(got, ref, c, o)
     assert rel_err(ctx.get_vec(dev[0]), host[0]) <= 1e-10
+
+
+@pytest.mark.parametrize("integrator", ["SSPRK33", "SSPRK104", "KennedyCarpenterLewis2R54C", "CalvoFrancoRandez2R64",
+                                        "CarpenterKennedy2N54", "ToulorgeDesmet2N84F"])
+@pytest.mark.parametrize("real", ["double", "float"])
+def test_fused_hall_hod_steps_equal_kernel_lists_for_every_integrator(integrator, real):
+    # Hall + high-order dissipation (the curl kernel forms the dissipation sum) through every
+    # integrator's fused step, ping-pong buffers included, against the reference kernel lists
+    c = dict(order=6, testcase="hall_circular_wave", nodes=(12, 13, 14), lo=0.0, hi=TWO_PI_, periodic=True,
+             hall=True, dissipation="HIGH_ORDER", integrator=integrator, dt=0.005, real=real)
+    nf = NUM_FIELDS[integrator]
+    out = []
+    for kernel in ("AUTO", "LIST"):
+        ctx = maps_for(dict(c, stage_kernel=kernel)).context()
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b).astype(np.float64)
+        bh[: ctx.n, :3] += 1e-2 * np.random.default_rng(NOISE_SEED).standard_normal((ctx.n, 3))
+        dev = [ctx.vec(bh.astype(ctx.real)), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.time_steps(*dev, 3)
+        out.append([ctx.get_vec(dev[i]).astype(np.float64) for i in range(nf)] + [ctx.get_vec(dev[3]), 
+                   ctx.get_scalar(dev[6], n=2)])
+    scale = float(np.abs(out[1][0]).max())
+    for i in range(nf + 1):
+        # fields compared on the state's scale (b2 of the 2N schemes holds DT x DB)
+        e = float(np.abs(out[0][i] - out[1][i]).max()) / scale
+        assert e <= (1e-12 if real == "double" else 2e-6), (i, e)
+    np.testing.assert_allclose(out[0][-1], out[1][-1], rtol=1e-15 if real == "double" else 1e-6)
