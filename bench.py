@@ -479,6 +479,8 @@ def main() -> None:
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 / batched / precision lines")
     ap.add_argument("--stage-kernel", choices=("AUTO", "COLUMN", "BRICK"), default="AUTO",
                     help="kernels of the fused stages (IEQ_STAGE_KERNEL)")
+    ap.add_argument("--no-pairs", action="store_true",
+                    help="one node per thread in the Hall column kernels (IEQ_COL_PAIRS=0)")
     ap.add_argument("--sharded-batch", action="store_true",
                     help="only the batched form, its 32 solves split between the ranks")
     a = ap.parse_args()
@@ -517,6 +519,8 @@ def main() -> None:
         return
     m = maps()
     m.I_Tech["stage_kernel"] = a.stage_kernel
+    if a.no_pairs:
+        m.I_Tech["col_pairs"] = 0
     ctx = m.context(device=dev)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     nn = ctx.n
@@ -616,8 +620,8 @@ def main() -> None:
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     achieved = STAGE_BYTES_PER_NODE * nn / stage_avg / 1e9
-    roofline = {"bound": "hbm", "kernel": ("k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col") +
-                "<double, 6th classical, periodic, Hall, HOD, u=0> (fused CK2N54 a+b)",
+    kname = ("k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col" if a.no_pairs else "k_stage_hall_x2")
+    roofline = {"bound": "hbm", "kernel": kname + "<double, 6th classical, periodic, Hall, HOD, u=0> (fused CK2N54 a+b)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_src, "traffic": None,
                 "algorithmic_bytes_per_node": STAGE_BYTES_PER_NODE, "nodes_per_launch": nn,
@@ -629,7 +633,6 @@ def main() -> None:
                         "to the curl and stage kernels together"}
     # DRAM bytes (read + write) of one launch of the stage kernel, from the ncu capture
     # summarised in profiles/ ("traffic_bytes_per_launch: N" line of the kernel's summary)
-    kname = "k_stage_brick" if a.stage_kernel == "BRICK" else "k_stage_col"
     summary = os.path.join(ROOT, "profiles", f"{kname}_hall6_64cubed.md")
     if os.path.isfile(summary):
         with open(summary) as f:
@@ -644,7 +647,7 @@ def main() -> None:
         "ms_per_step": t_max / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (analytic whistler wave)",
         "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "rk_steps_per_step": NUM_STEPS_FULL,
-                   "stage_kernels": a.stage_kernel,
+                   "stage_kernels": a.stage_kernel, "nodes_per_thread": 1 if a.no_pairs else 2,
                    "stages_per_rk_step": STAGES, "step": "one full solve to t=0.5 (260 RK steps)",
                    "l2": L2_NOTE, "replicas": world},
         "e2e": {"value": e2e_value, "unit": "DOF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

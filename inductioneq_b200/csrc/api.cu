@@ -219,17 +219,27 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
   }
 }
 
+// the block shape of a column kernel (x, y, z threads; all zero: the default) and whether
+// the Hall kernels run two nodes per thread
+static ColShape col_shape(const int (&b)[3], bool pairs) {
+  ColShape sh;
+  if (b[0] > 0) sh = ColShape{b[0], b[1], b[2]};
+  sh.pairs = pairs;
+  return sh;
+}
+
 template <typename R>
 void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, bool hodp = false) {
   const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
   const bool foad = diss_kind(c->s) == DISS_FO_OR_AD;
+  const ColShape sh = col_shape(c->s.col_block, c->s.col_pairs);
   switch (c->op_id) {
-    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
-    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
-    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
-    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
-    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
-    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, foad, c->stream); break;
+    case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+    case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+    case 2: launch_stage_col<R, 2>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+    case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+    case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+    case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
   }
 }
 
@@ -253,13 +263,14 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
         a.Hint[s + i + RI] += (((R)op.minv[op.nb] * (R)op.DHO.at(op.nb, s + WH - 1)) * (R)op.DHO.at(op.nb, i)) * sgn;
   }
   const bool per = c->s.periodic;
+  const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs);
   switch (c->op_id) {
-    case 0: launch_curl_e<R, 0>(a, per, hod, c->stream); break;
-    case 1: launch_curl_e<R, 1>(a, per, hod, c->stream); break;
-    case 2: launch_curl_e<R, 2>(a, per, hod, c->stream); break;
-    case 3: launch_curl_e<R, 3>(a, per, hod, c->stream); break;
-    case 4: launch_curl_e<R, 4>(a, per, hod, c->stream); break;
-    case 5: launch_curl_e<R, 5>(a, per, hod, c->stream); break;
+    case 0: launch_curl_e<R, 0>(a, per, hod, sh, c->stream); break;
+    case 1: launch_curl_e<R, 1>(a, per, hod, sh, c->stream); break;
+    case 2: launch_curl_e<R, 2>(a, per, hod, sh, c->stream); break;
+    case 3: launch_curl_e<R, 3>(a, per, hod, sh, c->stream); break;
+    case 4: launch_curl_e<R, 4>(a, per, hod, sh, c->stream); break;
+    case 5: launch_curl_e<R, 5>(a, per, hod, sh, c->stream); break;
   }
 }
 
@@ -735,6 +746,14 @@ ieq_status ieq_create(ieq_ctx **out, const char *settings, const char *const *pa
   }
   c->op_id = (c->s.order / 2 - 1) + (c->s.extended ? 3 : 0);
   for (int a = 0; a < 3; ++a) {
+    // a periodic stencil wraps once: its half width (order / 2) must not exceed the nodes
+    // per direction minus one
+    if (c->s.periodic && c->s.nodes[a] < c->op.order / 2 + 1) {
+      g_create_error = "periodic NODES per direction must be at least order/2 + 1 = " +
+                       std::to_string(c->op.order / 2 + 1);
+      delete c;
+      return IEQ_ERR_SHAPE;
+    }
     if (!c->s.periodic && c->s.nodes[a] < 2 * c->op.nb) {
       g_create_error = "NODES per direction must be at least 2*NUM_BOUNDS = " + std::to_string(2 * c->op.nb);
       delete c;

@@ -42,6 +42,13 @@ struct Settings {
   // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN),
   // 4 LIST (no fusion: the reference's kernel list of each step on the caller's fields)
   int stage_kernel = 0;
+  // thread-block shapes of the column stage kernel (IEQ_COL_BLOCK=XxYxZ) and of the curl
+  // kernel (IEQ_CURL_BLOCK); X * Y * Z = 128, all zero for the default 32x4x1
+  int col_block[3] = {0, 0, 0};
+  int curl_block[3] = {0, 0, 0};
+  // IEQ_COL_PAIRS=0: the Hall column kernels keep one node per thread (default 1: two
+  // x-adjacent nodes per thread where nx and the field layout allow it)
+  bool col_pairs = true;
 };
 
 // parse helpers (settings.cpp)

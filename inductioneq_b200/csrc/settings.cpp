@@ -2,6 +2,7 @@
 // list (matlab/generate_settings.m:3-33, compute_numerical_solution_setup.m:57-137), and
 // expansion of the compact SBP coefficient tables.
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <sstream>
@@ -126,6 +127,20 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
       else if (val == "BRICK") s.stage_kernel = 3;
       else if (val == "LIST") s.stage_kernel = 4;
       else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE, BRICK or LIST"; return false; }
+    } else if (key == "IEQ_COL_BLOCK" || key == "IEQ_CURL_BLOCK") {
+      int *b = key == "IEQ_COL_BLOCK" ? s.col_block : s.curl_block;
+      char tail = 0;
+      if (std::sscanf(val.c_str(), "%dx%dx%d%c", &b[0], &b[1], &b[2], &tail) != 3 || b[0] < 1 || b[1] < 1 ||
+          b[2] < 1 || b[0] * b[1] * b[2] != 128) {
+        err = key + " must be XxYxZ with X * Y * Z = 128 (e.g. 32x4x1)";
+        return false;
+      }
+    } else if (key == "IEQ_COL_PAIRS") {
+      if (val != "0" && val != "1") {
+        err = "IEQ_COL_PAIRS must be 0 or 1";
+        return false;
+      }
+      s.col_pairs = val == "1";
     } else if (key == "USE_HALL") {
       s.hall = true;
     } else if (key == "USE_PERIODIC") {

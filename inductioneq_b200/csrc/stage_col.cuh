@@ -34,17 +34,9 @@ namespace ieq {
 #ifndef IEQ_CURL_NODES
 #define IEQ_CURL_NODES 1
 #endif
-#ifndef IEQ_COL_BX
-#define IEQ_COL_BX 32
-#endif
-#ifndef IEQ_COL_BY
-#define IEQ_COL_BY 4
-#endif
-#ifndef IEQ_COL_BZ
-#define IEQ_COL_BZ 1
-#endif
-constexpr int kColBX = IEQ_COL_BX, kColBY = IEQ_COL_BY, kColBZ = IEQ_COL_BZ;
-constexpr int kColThreads = kColBX * kColBY * kColBZ;
+// every column kernel runs 128-thread blocks; their x-y-z shape is a run-time choice
+// (ColShape), since the kernels index with blockDim
+constexpr int kColThreads = 128;
 constexpr int kColNodes = IEQ_COL_NODES;     // nodes per thread along z (stage kernel)
 constexpr int kCurlNodes = IEQ_CURL_NODES;   // nodes per thread along z (curl kernel)
 // the convection terms keep twelve sums per node and axis: one node per thread there
@@ -413,6 +405,65 @@ __global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ 
   }
 }
 
+// one axis of the curl at one node: the derivatives v1, v2 of the two components of B
+// orthogonal to the axis and, with HODS, the dissipation-row sum ho of all three (interior
+// row, periodic wrap or SBP boundary rows; each sum term by term in stencil order)
+template <typename R, int OP, bool PER, bool HODS>
+__device__ __forceinline__ void curl_axis_node(const CurlArgs<R, SoA<R>> &a, int ax, int i, int n, long long idx,
+                                               long long st, const V3<R> &Bm, R &v1, R &v2, V3<R> &ho) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
+  constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
+  const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+  v1 = 0;
+  v2 = 0;
+  ho = {0, 0, 0};
+  const int row = PER ? NB : sbp_row(i, n, NB);
+  if (row == NB) {
+    const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+    for (int o = -RI; o <= RI; ++o) {
+      const R cH = a.Hint[o + RI];
+      if (o == 0) {
+        if (HODS) {
+          ho.x += cH * Bm.x; ho.y += cH * Bm.y; ho.z += cH * Bm.z;
+        }
+        continue;
+      }
+      const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st : idx + (long long)o * st;
+      const R c = a.Dint[o + RI];
+      if (HODS) {
+        const V3<R> B = ldf(a.b, j);
+        v1 += c * cmp(B, c1);
+        v2 += c * cmp(B, c2);
+        ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
+      } else {
+        v1 += c * __ldg(a.b.p + j + c1 * a.b.s);
+        v2 += c * __ldg(a.b.p + j + c2 * a.b.s);
+      }
+    }
+  } else {
+    for (int o = -RB; o <= RB; ++o) {
+      const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+      const R cH = (HODS && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+      if (cD == (R)0 && cH == (R)0) continue;
+      const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st;
+      if (HODS) {
+        const V3<R> B = ldf(a.b, j);
+        if (cD != (R)0) {
+          v1 += cD * cmp(B, c1);
+          v2 += cD * cmp(B, c2);
+        }
+        if (cH != (R)0) {
+          ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
+        }
+      } else {
+        v1 += cD * __ldg(a.b.p + j + c1 * a.b.s);
+        v2 += cD * __ldg(a.b.p + j + c2 * a.b.s);
+      }
+    }
+  }
+}
+
 // J = curl(B)/rho, E = J x B and, for the dissipation of the next stage kernel, the sum over
 // the axes of the dissipation rows of B (one node per thread).  Every axis loads all three
 // components of B at its stencil points once: the two orthogonal components feed the curl,
@@ -426,8 +477,6 @@ __global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ 
 template <typename R, int OP, bool PER>
 __global__ void __launch_bounds__(kColThreads, IEQ_CURL_MIN_BLOCKS * 128 / kColThreads)
     k_curl_e_hod(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
-  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
-  constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -443,42 +492,9 @@ __global__ void __launch_bounds__(kColThreads, IEQ_CURL_MIN_BLOCKS * 128 / kColT
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
     const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
-    R v1 = 0, v2 = 0;
-    V3<R> ho = {0, 0, 0};
-    const int i = ii[ax], n = nn[ax];
-    const int row = PER ? NB : sbp_row(i, n, NB);
-    if (row == NB) {
-      const bool wrap = PER && (i < RI || i >= n - RI);
-#pragma unroll
-      for (int o = -RI; o <= RI; ++o) {
-        const R cH = a.Hint[o + RI];
-        if (o == 0) {
-          ho.x += cH * Bm.x; ho.y += cH * Bm.y; ho.z += cH * Bm.z;
-          continue;
-        }
-        const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
-        const V3<R> B = ldf(a.b, j);
-        const R c = a.Dint[o + RI];
-        v1 += c * cmp(B, c1);
-        v2 += c * cmp(B, c2);
-        ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
-      }
-    } else {
-      for (int o = -RB; o <= RB; ++o) {
-        const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
-        const R cH = (o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
-        if (cD == (R)0 && cH == (R)0) continue;
-        const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
-        const V3<R> B = ldf(a.b, j);
-        if (cD != (R)0) {
-          v1 += cD * cmp(B, c1);
-          v2 += cD * cmp(B, c2);
-        }
-        if (cH != (R)0) {
-          ho.x += cH * B.x; ho.y += cH * B.y; ho.z += cH * B.z;
-        }
-      }
-    }
+    R v1, v2;
+    V3<R> ho;
+    curl_axis_node<R, OP, PER, true>(a, ax, ii[ax], nn[ax], idx, st[ax], Bm, v1, v2, ho);
     g[ax][c1] = v1 * a.inv_d[ax];
     g[ax][c2] = v2 * a.inv_d[ax];
     hod.x += ho.x; hod.y += ho.y; hod.z += ho.z;
@@ -515,19 +531,24 @@ __global__ void k_soa_ssp104_06(long long n, SoA<R> b1, SoA<R> b2, SoA<R> b3, R 
   }
 }
 
-// launch shape of the column kernels: kColBX x kColBY x kColBZ threads (kColThreads), each
-// `nodes` nodes in z
-inline dim3 col_block() { return dim3(kColBX, kColBY, kColBZ); }
-inline dim3 col_grid(int nx, int ny, int nz, int nodes) {
-  const int zb = kColBZ * nodes;
-  return dim3((unsigned)((nx + kColBX - 1) / kColBX), (unsigned)((ny + kColBY - 1) / kColBY),
-              (unsigned)((nz + zb - 1) / zb));
+// launch shape of the column kernels: x * y * z == kColThreads threads, each `nodes` nodes
+// in z.  32 x 4 x 1 keeps every warp on one x row (two full 128-byte lines per FP64 load).
+// pairs: the Hall kernels that have the form (stage_x2.cuh) give each thread two
+// x-adjacent nodes where the fields allow it.
+struct ColShape {
+  int x = 32, y = 4, z = 1;
+  bool pairs = true;
+};
+inline dim3 col_block(ColShape sh) { return dim3((unsigned)sh.x, (unsigned)sh.y, (unsigned)sh.z); }
+inline dim3 col_grid(ColShape sh, int nx, int ny, int nz, int nodes) {
+  const int zb = sh.z * nodes;
+  return dim3((unsigned)((nx + sh.x - 1) / sh.x), (unsigned)((ny + sh.y - 1) / sh.y), (unsigned)((nz + zb - 1) / zb));
 }
 
 template <typename R, int OP>
 void launch_stage_col(const StageArgs<R, SoA<R>> &a, bool per, bool hall, bool hod, int conv, bool hodp,
-                      bool foad, cudaStream_t s);
+                      bool foad, ColShape sh, cudaStream_t s);
 template <typename R, int OP>
-void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, bool hod, cudaStream_t s);
+void launch_curl_e(const CurlArgs<R, SoA<R>> &a, bool per, bool hod, ColShape sh, cudaStream_t s);
 
 }  // namespace ieq

@@ -2,6 +2,7 @@
 // both field layouts.  Included by stage_<real>_o<op>.cu with IEQ_R and IEQ_OP defined, so
 // the instantiations compile in parallel.
 #include "stage_brick.cuh"
+#include "stage_x2.cuh"
 
 namespace ieq {
 
@@ -84,10 +85,23 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
 
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
-                                     bool hodp, bool foad, cudaStream_t s) {
-  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block();
+                                     bool hodp, bool foad, ColShape sh, cudaStream_t s) {
+  const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block(sh);
   // the precomputed dissipation sum comes with the Hall curl kernel only
   hodp = hodp && hall && hod && !foad;
+  if (sh.pairs && hall && !conv && !foad && (hodp || !hod) && a.m.nx % 2 == 0 && pair_ok(a.E) &&
+      pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
+      pair_ok(a.out3)) {
+    const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
+    if (per) {
+      if (hodp) k_stage_hall_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
+      else k_stage_hall_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
+    } else {
+      if (hodp) k_stage_hall_x2<IEQ_R, IEQ_OP, false, true><<<g2, b, 0, s>>>(a);
+      else k_stage_hall_x2<IEQ_R, IEQ_OP, false, false><<<g2, b, 0, s>>>(a);
+    }
+    return;
+  }
   if (per) {
     if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, foad, g, b, s);
     else launch_col_ph<true, false>(a, hod, conv, false, foad, g, b, s);
@@ -98,15 +112,28 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
 }
 
 template <>
-void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hod, cudaStream_t s) {
-  const dim3 b = col_block();
+void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hod, ColShape sh,
+                                  cudaStream_t s) {
+  const dim3 b = col_block(sh);
+  if (sh.pairs && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
+      (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
+    const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
+    if (hod) {
+      if (per) k_curl_e_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
+      else k_curl_e_x2<IEQ_R, IEQ_OP, false, true><<<g2, b, 0, s>>>(a);
+    } else {
+      if (per) k_curl_e_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
+      else k_curl_e_x2<IEQ_R, IEQ_OP, false, false><<<g2, b, 0, s>>>(a);
+    }
+    return;
+  }
   if (hod) {
-    const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, 1);
+    const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, 1);
     if (per) k_curl_e_hod<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
     else k_curl_e_hod<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
     return;
   }
-  const dim3 g = col_grid(a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
+  const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
   if (per) k_curl_e<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
   else k_curl_e<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
 }

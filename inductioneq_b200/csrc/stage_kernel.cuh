@@ -329,42 +329,62 @@ __device__ __forceinline__ EpIn<R> epilogue_load(const StageArgs<R, F> &a, long 
   return e;
 }
 
+// the values a mode stores: o1 into out, o2 into out2 (fused 2N / 2R modes), o3 into out3
+// (EP_2R_FUSED, if set)
+template <typename R>
+struct EpOut {
+  V3<R> o1, o2, o3;
+};
+__host__ __device__ constexpr bool epilogue_writes_out2(int mode) {
+  return mode == EP_2N_FUSED || mode == EP_2N_FUSED_FIRST || mode == EP_2R_FUSED;
+}
+
 template <typename R, typename F>
-__device__ __forceinline__ void epilogue_store(const StageArgs<R, F> &a, long long idx, const V3<R> &db,
-                                               const EpIn<R> &e) {
+__device__ __forceinline__ EpOut<R> epilogue_values(const StageArgs<R, F> &a, const V3<R> &db, const EpIn<R> &e) {
   const V3<R> &X = e.X, &Y = e.Y;
+  EpOut<R> r = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   switch (a.mode) {
     case EP_X_PLUS_HF:
-      stf(a.out, idx, V3<R>{X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z});
+      r.o1 = V3<R>{X.x + a.h * db.x, X.y + a.h * db.y, X.z + a.h * db.z};
       break;
     case EP_PX_QYHF:
-      stf(a.out, idx, V3<R>{a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
-                            a.p * X.z + a.q * (Y.z + a.h * db.z)});
+      r.o1 = V3<R>{a.p * X.x + a.q * (Y.x + a.h * db.x), a.p * X.y + a.q * (Y.y + a.h * db.y),
+                   a.p * X.z + a.q * (Y.z + a.h * db.z)};
       break;
     case EP_HF:
-      stf(a.out, idx, V3<R>{a.h * db.x, a.h * db.y, a.h * db.z});
+      r.o1 = V3<R>{a.h * db.x, a.h * db.y, a.h * db.z};
       break;
     case EP_AX_HF:
-      stf(a.out, idx, V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z});
+      r.o1 = V3<R>{a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
       break;
     case EP_2N_FUSED:
     case EP_2N_FUSED_FIRST: {
       V3<R> t;
       if (a.mode == EP_2N_FUSED) t = {a.A * X.x + a.h * db.x, a.A * X.y + a.h * db.y, a.A * X.z + a.h * db.z};
       else t = {a.h * db.x, a.h * db.y, a.h * db.z};
-      stf(a.out, idx, t);
-      stf(a.out2, idx, V3<R>{Y.x + a.Bc * t.x, Y.y + a.Bc * t.y, Y.z + a.Bc * t.z});
+      r.o1 = t;
+      r.o2 = V3<R>{Y.x + a.Bc * t.x, Y.y + a.Bc * t.y, Y.z + a.Bc * t.z};
       break;
     }
     case EP_2R_FUSED: {
       const V3<R> t = {a.h * db.x, a.h * db.y, a.h * db.z};
       const V3<R> o = {X.x + a.A * t.x, X.y + a.A * t.y, X.z + a.A * t.z};
-      stf(a.out, idx, o);
-      stf(a.out2, idx, V3<R>{o.x + a.Bc * t.x, o.y + a.Bc * t.y, o.z + a.Bc * t.z});
-      if (a.out3.p) stf(a.out3, idx, t);
+      r.o1 = o;
+      r.o2 = V3<R>{o.x + a.Bc * t.x, o.y + a.Bc * t.y, o.z + a.Bc * t.z};
+      r.o3 = t;
       break;
     }
   }
+  return r;
+}
+
+template <typename R, typename F>
+__device__ __forceinline__ void epilogue_store(const StageArgs<R, F> &a, long long idx, const V3<R> &db,
+                                               const EpIn<R> &e) {
+  const EpOut<R> r = epilogue_values(a, db, e);
+  stf(a.out, idx, r.o1);
+  if (epilogue_writes_out2(a.mode)) stf(a.out2, idx, r.o2);
+  if (a.mode == EP_2R_FUSED && a.out3.p) stf(a.out3, idx, r.o3);
 }
 
 template <typename R, typename F>

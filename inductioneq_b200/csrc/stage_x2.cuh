@@ -1,0 +1,436 @@
+// stage_x2.cuh -- the Hall column kernels with two x-adjacent nodes per thread.
+//
+// The two kernels of a Hall stage (the curl kernel J = curl(B)/rho, E = J x B and the
+// dissipation sum H; the stage kernel gathering the flux rows on E) are bound by load
+// issue and load latency, not by DRAM bandwidth, at the sizes of this path: the FP32
+// build, with half the bytes, is only a few per cent faster.  Here each thread owns the
+// nodes (ix, ix + 1), ix even.  Every y and z stencil point of both nodes comes from one
+// pair load (16 bytes in FP64), and the x stencils of both nodes from 2*QL+1 pair loads
+// covering ix-2QL .. ix+2QL+1 (QL = ceil(RI/2)), instead of two scalar loads per point and
+// node: about half the load instructions and address arithmetic per node.
+//
+// Each node's sums are formed term by term in the order of the one-node kernels
+// (k_curl_e, k_curl_e_hod, k_stage_col), so the results are the same.
+//
+// A launcher uses these kernels only when every pair is aligned and stays in one row:
+// nx even, each field's component stride even and its base aligned to two elements.
+// x-boundary rows of a non-periodic box (and pairs whose x window would leave the row)
+// take the one-node code per node.
+#pragma once
+#include "stage_col.cuh"
+
+namespace ieq {
+
+template <typename R>
+struct Pair2;
+template <>
+struct Pair2<double> {
+  using T = double2;
+};
+template <>
+struct Pair2<float> {
+  using T = float2;
+};
+
+// the values at j and j + 1 (j even) through the read-only path
+template <typename R>
+__device__ __forceinline__ void ld_pair(const R *p, R &v0, R &v1) {
+  const typename Pair2<R>::T v = __ldg(reinterpret_cast<const typename Pair2<R>::T *>(p));
+  v0 = v.x;
+  v1 = v.y;
+}
+// the same through the ordinary path (fields the kernel also writes)
+template <typename R>
+__device__ __forceinline__ void ld_pair_plain(const R *p, R &v0, R &v1) {
+  const typename Pair2<R>::T v = *reinterpret_cast<const typename Pair2<R>::T *>(p);
+  v0 = v.x;
+  v1 = v.y;
+}
+template <typename R>
+__device__ __forceinline__ void st_pair(R *p, R v0, R v1) {
+  typename Pair2<R>::T v;
+  v.x = v0;
+  v.y = v1;
+  *reinterpret_cast<typename Pair2<R>::T *>(p) = v;
+}
+template <typename R>
+__device__ __forceinline__ void ldf_pair(const SoA<R> &f, long long j, V3<R> &a, V3<R> &b) {
+  ld_pair(f.p + j, a.x, b.x);
+  ld_pair(f.p + j + f.s, a.y, b.y);
+  ld_pair(f.p + j + 2 * f.s, a.z, b.z);
+}
+template <typename R>
+__device__ __forceinline__ void ldf_pair_plain(const SoA<R> &f, long long j, V3<R> &a, V3<R> &b) {
+  ld_pair_plain(f.p + j, a.x, b.x);
+  ld_pair_plain(f.p + j + f.s, a.y, b.y);
+  ld_pair_plain(f.p + j + 2 * f.s, a.z, b.z);
+}
+template <typename R>
+__device__ __forceinline__ void stf_pair(const SoA<R> &f, long long j, const V3<R> &a, const V3<R> &b) {
+  st_pair(f.p + j, a.x, b.x);
+  st_pair(f.p + j + f.s, a.y, b.y);
+  st_pair(f.p + j + 2 * f.s, a.z, b.z);
+}
+template <typename R>
+__device__ __forceinline__ R &cref(V3<R> &v, int c) {
+  return c == 0 ? v.x : (c == 1 ? v.y : v.z);
+}
+
+// the x window of one component for the pair at (row0 + ix, row0 + ix + 1):
+// w[m] = f[row0 + ix - 2QL + m], m = 0 .. 4QL+1, periodic wrap of the pair starts
+template <typename R, int QL, bool PER>
+__device__ __forceinline__ void x_window(const R *f, long long row0, int ix, int nx, R (&w)[4 * QL + 2]) {
+#pragma unroll
+  for (int q = -QL; q <= QL; ++q) {
+    int xx = ix + 2 * q;
+    if (PER) {
+      xx += xx < 0 ? nx : 0;
+      xx -= xx >= nx ? nx : 0;
+    }
+    ld_pair(f + row0 + xx, w[2 * (q + QL)], w[2 * (q + QL) + 1]);
+  }
+}
+
+// whether the pair's x stencils may use the window (both nodes on the interior row and
+// the window inside the row; always with periodic wrap)
+template <int OP, bool PER>
+__device__ __forceinline__ bool x_pair_interior(int ix, int nx) {
+  constexpr int NB = Op<OP>::NB, QL = (Op<OP>::RI + 1) / 2;
+  if (PER) return true;
+  return sbp_row(ix, nx, NB) == NB && sbp_row(ix + 1, nx, NB) == NB && ix - 2 * QL >= 0 && ix + 2 * QL + 1 < nx;
+}
+
+// resident 128-thread blocks per SM the register allocation targets (measured on B200 at
+// 64^3 and 128^3, FP64: the curl kernel is fastest with 4 blocks of <= 128 registers and
+// no spills, 15-25 % ahead of 5 or 6 blocks with spills; the stage kernel with 8 blocks of
+// <= 64 registers)
+#ifndef IEQ_CURL_X2_MIN_BLOCKS
+#define IEQ_CURL_X2_MIN_BLOCKS 4
+#endif
+#ifndef IEQ_STAGE_X2_MIN_BLOCKS
+#define IEQ_STAGE_X2_MIN_BLOCKS 8
+#endif
+
+// J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at the pair of nodes
+template <typename R, int OP, bool PER, bool HODS>
+__global__ void __launch_bounds__(kColThreads, IEQ_CURL_X2_MIN_BLOCKS)
+    k_curl_e_x2(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
+  constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
+  constexpr int QL = (RI + 1) / 2;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix >= nx || iy >= ny || iz >= nz) return;
+  const long long row0 = (long long)nx * (iy + (long long)ny * iz);
+  const long long idx = row0 + ix;
+  const long long cs = a.b.s;
+  const V3<R> zero = {0, 0, 0};
+  V3<R> Bm[2];
+  ldf_pair(a.b, idx, Bm[0], Bm[1]);
+  R g[2][3][3];
+  V3<R> hod[2] = {zero, zero};
+
+  // x
+  {
+    R v1[2], v2[2];
+    V3<R> ho[2];
+    if (x_pair_interior<OP, PER>(ix, nx)) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        v1[k] = 0;
+        v2[k] = 0;
+        ho[k] = zero;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!HODS && c == 0) continue;   // the x derivatives of By and Bz only
+        R w[4 * QL + 2];
+        x_window<R, QL, PER>(a.b.p + c * cs, row0, ix, nx, w);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+#pragma unroll
+          for (int o = -RI; o <= RI; ++o) {
+            const R val = w[2 * QL + k + o];
+            if (o != 0) {
+              if (c == 1) v1[k] += a.Dint[o + RI] * val;
+              if (c == 2) v2[k] += a.Dint[o + RI] * val;
+            }
+            if (HODS) cref(ho[k], c) += a.Hint[o + RI] * val;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        curl_axis_node<R, OP, PER, HODS>(a, 0, ix + k, nx, idx + k, 1, Bm[k], v1[k], v2[k], ho[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      g[k][0][1] = v1[k] * a.inv_d[0];
+      g[k][0][2] = v2[k] * a.inv_d[0];
+      if (HODS) {
+        hod[k].x += ho[k].x; hod[k].y += ho[k].y; hod[k].z += ho[k].z;
+      }
+    }
+  }
+
+  // y and z: both nodes on the same row of the axis
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {nx, ny, nz};
+  const long long st[3] = {1, nx, (long long)nx * ny};
+#pragma unroll
+  for (int ax = 1; ax < 3; ++ax) {
+    const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+    const int i = ii[ax], n = nn[ax];
+    R v1[2] = {0, 0}, v2[2] = {0, 0};
+    V3<R> ho[2] = {zero, zero};
+    const int row = PER ? NB : sbp_row(i, n, NB);
+    if (row == NB) {
+      const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) {
+        const R cH = a.Hint[o + RI];
+        if (o == 0) {
+          if (HODS) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+              ho[k].x += cH * Bm[k].x; ho[k].y += cH * Bm[k].y; ho[k].z += cH * Bm[k].z;
+            }
+          }
+          continue;
+        }
+        const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
+        const R c = a.Dint[o + RI];
+        if (HODS) {
+          V3<R> B[2];
+          ldf_pair(a.b, j, B[0], B[1]);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            v1[k] += c * cmp(B[k], c1);
+            v2[k] += c * cmp(B[k], c2);
+            ho[k].x += cH * B[k].x; ho[k].y += cH * B[k].y; ho[k].z += cH * B[k].z;
+          }
+        } else {
+          R p1[2], p2[2];
+          ld_pair(a.b.p + j + c1 * cs, p1[0], p1[1]);
+          ld_pair(a.b.p + j + c2 * cs, p2[0], p2[1]);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            v1[k] += c * p1[k];
+            v2[k] += c * p2[k];
+          }
+        }
+      }
+    } else {
+      for (int o = -RB; o <= RB; ++o) {
+        const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+        const R cH = (HODS && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+        if (cD == (R)0 && cH == (R)0) continue;
+        const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
+        if (HODS) {
+          V3<R> B[2];
+          ldf_pair(a.b, j, B[0], B[1]);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            if (cD != (R)0) {
+              v1[k] += cD * cmp(B[k], c1);
+              v2[k] += cD * cmp(B[k], c2);
+            }
+            if (cH != (R)0) {
+              ho[k].x += cH * B[k].x; ho[k].y += cH * B[k].y; ho[k].z += cH * B[k].z;
+            }
+          }
+        } else {
+          R p1[2], p2[2];
+          ld_pair(a.b.p + j + c1 * cs, p1[0], p1[1]);
+          ld_pair(a.b.p + j + c2 * cs, p2[0], p2[1]);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            v1[k] += cD * p1[k];
+            v2[k] += cD * p2[k];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      g[k][ax][c1] = v1[k] * a.inv_d[ax];
+      g[k][ax][c2] = v2[k] * a.inv_d[ax];
+      if (HODS) {
+        hod[k].x += ho[k].x; hod[k].y += ho[k].y; hod[k].z += ho[k].z;
+      }
+    }
+  }
+
+  R r[2] = {1, 1};
+  if (a.rho) ld_pair(a.rho + idx, r[0], r[1]);
+  V3<R> E[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    V3<R> J = {g[k][1][2] - g[k][2][1], g[k][2][0] - g[k][0][2], g[k][0][1] - g[k][1][0]};
+    if (a.rho) {
+      const R ri = (R)1 / r[k];
+      J = {J.x * ri, J.y * ri, J.z * ri};
+    }
+    const V3<R> &B = Bm[k];
+    E[k] = V3<R>{J.x * B.y - J.y * B.x, J.x * B.z - J.z * B.x, J.y * B.z - J.z * B.y};
+    if (!PER && (ix + k == 0 || iy == 0 || iz == 0 || ix + k == nx - 1 || iy == ny - 1 || iz == nz - 1))
+      stf(a.jface, idx + k, J);
+  }
+  stf_pair(a.out, idx, E[0], E[1]);
+  if (HODS) stf_pair(a.hout, idx, hod[0], hod[1]);
+}
+
+// the stage update of the pair from DB (epilogue modes of stage_kernel.cuh), with pair loads
+// and stores of the fields it combines
+template <typename R>
+__device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
+                                                    const V3<R> &d1) {
+  EpIn<R> e[2];
+  const V3<R> zero = {0, 0, 0};
+  e[0] = EpIn<R>{zero, zero};
+  e[1] = e[0];
+  switch (a.mode) {
+    case EP_X_PLUS_HF:
+    case EP_AX_HF:
+    case EP_2R_FUSED:
+      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
+      break;
+    case EP_PX_QYHF:
+      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
+      ldf_pair_plain(a.Y, idx, e[0].Y, e[1].Y);
+      break;
+    case EP_2N_FUSED:
+      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
+      ldf_pair_plain(a.Z, idx, e[0].Y, e[1].Y);
+      break;
+    case EP_2N_FUSED_FIRST:
+      ldf_pair_plain(a.Z, idx, e[0].Y, e[1].Y);
+      break;
+    default:
+      break;
+  }
+  const EpOut<R> o0 = epilogue_values(a, d0, e[0]), o1 = epilogue_values(a, d1, e[1]);
+  stf_pair(a.out, idx, o0.o1, o1.o1);
+  if (epilogue_writes_out2(a.mode)) stf_pair(a.out2, idx, o0.o2, o1.o2);
+  if (a.mode == EP_2R_FUSED && a.out3.p) stf_pair(a.out3, idx, o0.o3, o1.o3);
+}
+
+// DB of a Hall stage without convection terms at the pair, with the dissipation sum
+// precomputed (HODP, read from a.Hpre) or absent, and the stage update
+template <typename R, int OP, bool PER, bool HODP>
+__global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
+    k_stage_hall_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
+  constexpr int QL = (RI + 1) / 2;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix < nx && iy < ny && iz < nz) {
+    const long long row0 = (long long)nx * (iy + (long long)ny * iz);
+    const long long idx = row0 + ix;
+    const long long es = a.E.s;
+    const V3<R> zero = {0, 0, 0};
+    V3<R> db[2] = {zero, zero};
+
+    // x: DB_y += D[Exy], DB_z += D[Exz]
+    {
+      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
+      if (x_pair_interior<OP, PER>(ix, nx)) {
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+          R w[4 * QL + 2];
+          x_window<R, QL, PER>(a.E.p + (ci == 0 ? e_comp1(0) : e_comp2(0)) * es, row0, ix, nx, w);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+#pragma unroll
+            for (int o = -RI; o <= RI; ++o) {
+              if (o == 0) continue;
+              if (ci == 0) s[k].h1 += a.Dint[o + RI] * w[2 * QL + k + o];
+              else s[k].h2 += a.Dint[o + RI] * w[2 * QL + k + o];
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          col_axis<R, OP, PER, true, false, 0>(s[k], a, 0, ix + k, nx, idx + k, 1, zero);
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) col_combine<R, true, false, 0>(a, 0, s[k], zero, zero, db[k], db[k]);
+    }
+
+    // y and z
+    const int ii[3] = {ix, iy, iz};
+    const int nn[3] = {nx, ny, nz};
+    const long long st[3] = {1, nx, (long long)nx * ny};
+#pragma unroll
+    for (int ax = 1; ax < 3; ++ax) {
+      const int i = ii[ax], n = nn[ax];
+      const R *e1p = a.E.p + e_comp1(ax) * es, *e2p = a.E.p + e_comp2(ax) * es;
+      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
+      const int row = PER ? NB : sbp_row(i, n, NB);
+      if (row == NB) {
+        const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+        for (int o = -RI; o <= RI; ++o) {
+          if (o == 0) continue;
+          const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
+          R p1[2], p2[2];
+          ld_pair(e1p + j, p1[0], p1[1]);
+          ld_pair(e2p + j, p2[0], p2[1]);
+          const R c = a.Dint[o + RI];
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            s[k].h1 += c * p1[k];
+            s[k].h2 += c * p2[k];
+          }
+        }
+      } else {
+        for (int o = -C0; o <= C0; ++o) {
+          const R cD = a.tab->D[row][o + C0];
+          if (cD == (R)0) continue;
+          const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
+          R p1[2], p2[2];
+          ld_pair(e1p + j, p1[0], p1[1]);
+          ld_pair(e2p + j, p2[0], p2[1]);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            s[k].h1 += cD * p1[k];
+            s[k].h2 += cD * p2[k];
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) col_combine<R, true, false, 0>(a, ax, s[k], zero, zero, db[k], db[k]);
+    }
+
+    V3<R> hv[2] = {zero, zero};
+    if (HODP) ldf_pair(a.Hpre, idx, hv[0], hv[1]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (!PER) {
+        const int iik[3] = {ix + k, iy, iz};
+        stage_sat<R, SoA<R>, true>(a, iik, nn, idx + k, ldf(a.bk, idx + k), zero, 0, db[k]);
+      }
+      if (HODP) {
+        db[k].x += a.hod_factor * hv[k].x;
+        db[k].y += a.hod_factor * hv[k].y;
+        db[k].z += a.hod_factor * hv[k].z;
+      }
+    }
+    stage_epilogue_pair(a, idx, db[0], db[1]);
+  }
+  stage_time_post(a);
+}
+
+// whether a launch may use the pair kernels: nx even and every pair load or store aligned
+template <typename R>
+inline bool pair_ok(const SoA<R> &f) {
+  return f.p == nullptr || ((reinterpret_cast<uintptr_t>(f.p) % (2 * sizeof(R))) == 0 && f.s % 2 == 0);
+}
+
+}  // namespace ieq

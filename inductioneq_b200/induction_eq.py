@@ -106,6 +106,11 @@ class Maps:
         s += f" -DTC_OMEGA={self.tc_omega:.16e}"
         if self.I_Tech.get("stage_kernel", "AUTO") != "AUTO":
             s += f" -DIEQ_STAGE_KERNEL={self.I_Tech['stage_kernel']}"
+        for key, name in (("col_block", "IEQ_COL_BLOCK"), ("curl_block", "IEQ_CURL_BLOCK")):
+            if self.I_Tech.get(key):   # (x, y, z) threads of that column kernel, x * y * z = 128
+                s += f" -D{name}=" + "x".join(str(int(v)) for v in self.I_Tech[key])
+        if self.I_Tech.get("col_pairs") is not None:   # Hall column kernels: two nodes per thread
+            s += f" -DIEQ_COL_PAIRS={int(bool(self.I_Tech['col_pairs']))}"
         return s
 
     def kernel_path_list(self) -> list[str]:

@@ -477,3 +477,57 @@ def test_fused_hall_hod_steps_equal_kernel_lists_for_every_integrator(integrator
         e = float(np.abs(out[0][i] - out[1][i]).max()) / scale
         assert e <= (1e-12 if real == "double" else 2e-6), (i, e)
     np.testing.assert_allclose(out[0][-1], out[1][-1], rtol=1e-15 if real == "double" else 1e-6)
+
+
+@pytest.mark.parametrize("shape", [(128, 1, 1), (16, 4, 2), (8, 4, 4), (4, 8, 4)])
+@pytest.mark.parametrize("case", ["hall_hod_box", "rotation_conv"])
+def test_column_block_shape_does_not_change_the_result(shape, case):
+    # the block shape only regroups nodes: every node's arithmetic is the same, so the
+    # fields agree bit for bit (ragged grids: partial blocks in every direction)
+    if case == "hall_hod_box":
+        c = dict(order=6, testcase="hall_travelling_wave", nodes=(19, 13, 14), lo=0.0, hi=TWO_PI_, hall=True,
+                 dissipation="HIGH_ORDER", integrator="CarpenterKennedy2N54", dt=0.002)
+    else:
+        c = dict(order=4, testcase="rotation_gaussian", nodes=(21, 10, 9), lo=-1.0, hi=1.0, integrator="SSPRK33", dt=0.01)
+    out = []
+    for sh in (None, shape):
+        ctx = maps_for(dict(c, col_block=sh, curl_block=sh)).context()
+        dev = [ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.kernel("init_b", dev[0])
+        ctx.kernel("init_u", dev[4])
+        ctx.time_steps(*dev, 4)
+        out.append(ctx.get_vec(dev[0]))
+    assert np.array_equal(out[0], out[1])
+    assert np.isfinite(out[0]).all() and np.abs(out[0]).max() > 0
+
+
+@pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32"])
+def test_two_nodes_per_thread_equal_one_node_per_thread(case):
+    # the Hall column kernels with two x-adjacent nodes per thread form every node's sums in
+    # the order of the one-node kernels: the fields agree up to the compiler's choice of
+    # fused multiply-adds (a few units in the last place)
+    c = dict(order=6, testcase="hall_circular_wave", nodes=(18, 13, 14), lo=0.0, hi=TWO_PI_, hall=True,
+             integrator="CarpenterKennedy2N54", dt=0.002)
+    if case.startswith("periodic"):
+        c.update(periodic=True, nodes=(14, 12, 16))
+    if case.endswith("hod"):
+        c.update(dissipation="HIGH_ORDER")
+    if case.endswith("f32"):
+        c.update(real="float")
+    if case.startswith("box"):
+        c.update(testcase="hall_travelling_wave")
+    out = []
+    for pairs in (0, 1):
+        ctx = maps_for(dict(c, col_pairs=pairs)).context()
+        dev = [ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.kernel("init_b", dev[0])
+        ctx.time_steps(*dev, 3)
+        out.append([ctx.get_vec(dev[0]), ctx.get_vec(dev[1]), ctx.get_vec(dev[3])])
+    scale = float(np.abs(out[0][0]).max())
+    tol = 2e-6 if case.endswith("f32") else 1e-13
+    for i, (a, b) in enumerate(zip(*out)):
+        e = float(np.abs(a.astype(np.float64) - b).max()) / scale
+        assert e <= tol, (i, e)
+    assert np.isfinite(out[0][0]).all()
