@@ -102,13 +102,14 @@ __device__ __forceinline__ bool x_pair_interior(int ix, int nx) {
 
 // resident 128-thread blocks per SM the register allocation targets (measured on B200 at
 // 64^3 and 128^3, FP64: the curl kernel is fastest with 4 blocks of <= 128 registers and
-// no spills, 15-25 % ahead of 5 or 6 blocks with spills; the stage kernel with 8 blocks of
-// <= 64 registers)
+// no spills, 15-25 % ahead of 5 or 6 blocks with spills; the stage kernel with 7 blocks of
+// <= 72 registers, 3-7 % ahead of 8 blocks of 64 -- at 64^3 its 1024 blocks then fit in one
+// wave of 148 x 7)
 #ifndef IEQ_CURL_X2_MIN_BLOCKS
 #define IEQ_CURL_X2_MIN_BLOCKS 4
 #endif
 #ifndef IEQ_STAGE_X2_MIN_BLOCKS
-#define IEQ_STAGE_X2_MIN_BLOCKS 8
+#define IEQ_STAGE_X2_MIN_BLOCKS 7
 #endif
 
 // J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at the pair of nodes
@@ -286,9 +287,7 @@ __global__ void __launch_bounds__(kColThreads, IEQ_CURL_X2_MIN_BLOCKS)
 // the stage update of the pair from DB (epilogue modes of stage_kernel.cuh), with pair loads
 // and stores of the fields it combines
 template <typename R>
-__device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
-                                                    const V3<R> &d1) {
-  EpIn<R> e[2];
+__device__ __forceinline__ void epilogue_load_pair(const StageArgs<R, SoA<R>> &a, long long idx, EpIn<R> (&e)[2]) {
   const V3<R> zero = {0, 0, 0};
   e[0] = EpIn<R>{zero, zero};
   e[1] = e[0];
@@ -312,10 +311,21 @@ __device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &
     default:
       break;
   }
+}
+template <typename R>
+__device__ __forceinline__ void epilogue_store_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
+                                                    const V3<R> &d1, const EpIn<R> (&e)[2]) {
   const EpOut<R> o0 = epilogue_values(a, d0, e[0]), o1 = epilogue_values(a, d1, e[1]);
   stf_pair(a.out, idx, o0.o1, o1.o1);
   if (epilogue_writes_out2(a.mode)) stf_pair(a.out2, idx, o0.o2, o1.o2);
   if (a.mode == EP_2R_FUSED && a.out3.p) stf_pair(a.out3, idx, o0.o3, o1.o3);
+}
+template <typename R>
+__device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
+                                                    const V3<R> &d1) {
+  EpIn<R> e[2];
+  epilogue_load_pair(a, idx, e);
+  epilogue_store_pair(a, idx, d0, d1, e);
 }
 
 // DB of a Hall stage without convection terms at the pair, with the dissipation sum
