@@ -83,6 +83,25 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
   }
 }
 
+// the same with two x-adjacent nodes per thread (k_stage_col_x2)
+template <bool P, bool H>
+static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
+                             dim3 b, cudaStream_t s) {
+  if (foad) {
+    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1, false, true><<<g, b, 0, s>>>(a);
+    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0, false, true><<<g, b, 0, s>>>(a);
+  } else if (hod && hodp) {
+    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1, true><<<g, b, 0, s>>>(a);
+    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0, true><<<g, b, 0, s>>>(a);
+  } else if (hod) {
+    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1><<<g, b, 0, s>>>(a);
+    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0><<<g, b, 0, s>>>(a);
+  } else {
+    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1><<<g, b, 0, s>>>(a);
+    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0><<<g, b, 0, s>>>(a);
+  }
+}
+
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
                                      bool hodp, bool foad, ColShape sh, cudaStream_t s) {
@@ -102,6 +121,17 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
     }
     return;
   }
+  // the general pair kernel: periodic Hall runs (with convection or first-order / adaptive
+  // dissipation; measured 25-35 % faster there than one node per thread, whose Hall +
+  // convection build spills at 64 registers).  On boxes and without the Hall term the
+  // one-node kernels measured faster (the x boundary rows run per node, and the
+  // convection sums of two nodes exceed the registers).
+  if (sh.pairs && per && hall && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
+      pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
+      pair_ok(a.out3)) {
+    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1), b, s);
+    return;
+  }
   if (per) {
     if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, foad, g, b, s);
     else launch_col_ph<true, false>(a, hod, conv, false, foad, g, b, s);
@@ -115,16 +145,13 @@ template <>
 void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hod, ColShape sh,
                                   cudaStream_t s) {
   const dim3 b = col_block(sh);
-  if (sh.pairs && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
+  // pairs on periodic grids only (on boxes the x boundary rows run per node and the
+  // one-node kernels measured faster)
+  if (sh.pairs && per && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
       (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
     const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
-    if (hod) {
-      if (per) k_curl_e_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
-      else k_curl_e_x2<IEQ_R, IEQ_OP, false, true><<<g2, b, 0, s>>>(a);
-    } else {
-      if (per) k_curl_e_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
-      else k_curl_e_x2<IEQ_R, IEQ_OP, false, false><<<g2, b, 0, s>>>(a);
-    }
+    if (hod) k_curl_e_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
+    else k_curl_e_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
     return;
   }
   if (hod) {

@@ -108,13 +108,16 @@ __device__ __forceinline__ bool x_pair_interior(int ix, int nx) {
 #ifndef IEQ_CURL_X2_MIN_BLOCKS
 #define IEQ_CURL_X2_MIN_BLOCKS 4
 #endif
+#ifndef IEQ_CURL_X2_PLAIN_MIN_BLOCKS
+#define IEQ_CURL_X2_PLAIN_MIN_BLOCKS 8
+#endif
 #ifndef IEQ_STAGE_X2_MIN_BLOCKS
 #define IEQ_STAGE_X2_MIN_BLOCKS 7
 #endif
 
 // J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at the pair of nodes
 template <typename R, int OP, bool PER, bool HODS>
-__global__ void __launch_bounds__(kColThreads, IEQ_CURL_X2_MIN_BLOCKS)
+__global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : IEQ_CURL_X2_PLAIN_MIN_BLOCKS)
     k_curl_e_x2(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
@@ -430,6 +433,174 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
         db[k].x += a.hod_factor * hv[k].x;
         db[k].y += a.hod_factor * hv[k].y;
         db[k].z += a.hod_factor * hv[k].z;
+      }
+    }
+    stage_epilogue_pair(a, idx, db[0], db[1]);
+  }
+  stage_time_post(a);
+}
+
+// ---------------------------------------------------------------------------------------
+// The general column stage kernel (convection sums, dissipation gathered here or
+// precomputed, first-order / adaptive dissipation) with two x-adjacent nodes per thread.
+// The x stencils stream through the pairs at ix + 2q, q = -QL .. QL: the pair's first value
+// is offset 2q of node ix and offset 2q - 1 of node ix + 1, its second offsets 2q + 1 and 2q,
+// so each node meets its offsets in ascending order -- the order of col_axis -- without a
+// window kept in registers.  Every term goes through col_acc / col_combine, as in k_stage_col.
+
+// the stencil-point values col_load reads, for both nodes of a pair at j, j + 1
+template <typename R, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_load_pair(const StageArgs<R, SoA<R>> &a, int ax, long long j, V3<R> (&B)[2],
+                                              V3<R> (&U)[2], R (&e1)[2], R (&e2)[2]) {
+  if (CONV || HOD) ldf_pair(a.bk, j, B[0], B[1]);
+  if (CONV) ldf_pair(a.u, j, U[0], U[1]);
+  if (HALL) {
+    ld_pair(a.E.p + j + e_comp1(ax) * a.E.s, e1[0], e1[1]);
+    ld_pair(a.E.p + j + e_comp2(ax) * a.E.s, e2[0], e2[1]);
+  }
+}
+
+// the x sums of the pair (ix, ix + 1) on the interior row (or with periodic wrap)
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_x_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, long long row0, int ix,
+                                           int nx) {
+  constexpr int RI = Op<OP>::RI, QL = (RI + 1) / 2;
+  const int need = a.need;
+  const V3<R> zero = {0, 0, 0};
+#pragma unroll
+  for (int q = -QL; q <= QL; ++q) {
+    int xx = ix + 2 * q;
+    if (PER) {
+      xx += xx < 0 ? nx : 0;
+      xx -= xx >= nx ? nx : 0;
+    }
+    V3<R> B[2] = {zero, zero}, U[2] = {zero, zero};
+    R e1[2] = {0, 0}, e2[2] = {0, 0};
+    col_load_pair<R, HALL, HOD, CONV>(a, 0, row0 + xx, B, U, e1, e2);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int o = 2 * q + e - k;
+        if (o < -RI || o > RI) continue;
+        if (o == 0) {
+          // the interior derivative rows have a zero centre (the value is the node's own B)
+          if (HOD) col_acc<R, false, HOD, 0>(s[k], 0, 0, (R)0, a.Hint[RI], false, true, B[e], zero, (R)0, (R)0);
+          continue;
+        }
+        col_acc<R, HALL, HOD, CONV>(s[k], 0, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B[e], U[e], e1[e],
+                                    e2[e]);
+      }
+    }
+  }
+}
+
+// the y or z sums of the pair (both nodes on the same row of the axis)
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+__device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, int ax, int i, int n,
+                                            long long idx, long long st, const V3<R> (&Bm)[2]) {
+  constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
+  constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
+  const int need = a.need;
+  const V3<R> zero = {0, 0, 0};
+  const int row = PER ? NB : sbp_row(i, n, NB);
+  if (row == NB) {
+    const bool wrap = PER && (i < RI || i >= n - RI);
+#pragma unroll
+    for (int o = -RI; o <= RI; ++o) {
+      if (o == 0) {
+        if (HOD) {
+#pragma unroll
+          for (int k = 0; k < 2; ++k)
+            col_acc<R, false, HOD, 0>(s[k], ax, 0, (R)0, a.Hint[RI], false, true, Bm[k], zero, (R)0, (R)0);
+        }
+        continue;
+      }
+      const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st : idx + (long long)o * st;
+      V3<R> B[2] = {zero, zero}, U[2] = {zero, zero};
+      R e1[2] = {0, 0}, e2[2] = {0, 0};
+      col_load_pair<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        col_acc<R, HALL, HOD, CONV>(s[k], ax, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B[k], U[k], e1[k],
+                                    e2[k]);
+    }
+  } else {
+    for (int o = -RB; o <= RB; ++o) {
+      const R cD = (o >= -C0 && o <= C0) ? a.tab->D[row][o + C0] : (R)0;
+      const R cH = (HOD && o >= -(WH - 1) && o <= WH - 1) ? a.tab->H[row][o + WH - 1] : (R)0;
+      if (cD == (R)0 && cH == (R)0) continue;
+      const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st;
+      V3<R> B[2] = {zero, zero}, U[2] = {zero, zero};
+      R e1[2] = {0, 0}, e2[2] = {0, 0};
+      col_load_pair<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        col_acc<R, HALL, HOD, CONV>(s[k], ax, need, cD, cH, cD != (R)0, cH != (R)0, B[k], U[k], e1[k], e2[k]);
+    }
+  }
+}
+
+#ifndef IEQ_COL_X2_MIN_BLOCKS
+#define IEQ_COL_X2_MIN_BLOCKS 4
+#endif
+#ifndef IEQ_COL_X2_CONV_MIN_BLOCKS
+#define IEQ_COL_X2_CONV_MIN_BLOCKS 4
+#endif
+
+// DB (volume, Hall, SAT, dissipation) and the stage update at the pair; template
+// arguments as k_stage_col (CONV = 1: the convection sums; HODP: the dissipation sum read
+// from a.Hpre; FOAD: first-order / adaptive dissipation)
+template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false>
+__global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS)
+    k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+  constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ix < nx && iy < ny && iz < nz) {
+    const long long row0 = (long long)nx * (iy + (long long)ny * iz);
+    const long long idx = row0 + ix;
+    const V3<R> zero = {0, 0, 0};
+    V3<R> Bm[2], um[2] = {zero, zero}, db[2] = {zero, zero}, hod[2] = {zero, zero};
+    ldf_pair(a.bk, idx, Bm[0], Bm[1]);
+    if (CONV) ldf_pair(a.u, idx, um[0], um[1]);
+    {
+      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
+      if (x_pair_interior<OP, PER>(ix, nx)) {
+        col_x_pair<R, OP, PER, HALL, HOD, CONV>(s, a, row0, ix, nx);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          col_axis<R, OP, PER, HALL, HOD, CONV>(s[k], a, 0, ix + k, nx, idx + k, 1, Bm[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, 0, s[k], Bm[k], um[k], db[k], hod[k]);
+    }
+    const int nn[3] = {nx, ny, nz};
+    const long long st[3] = {1, nx, (long long)nx * ny};
+#pragma unroll
+    for (int ax = 1; ax < 3; ++ax) {
+      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
+      col_yz_pair<R, OP, PER, HALL, HOD, CONV>(s, a, ax, ax == 1 ? iy : iz, nn[ax], idx, st[ax], Bm);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, ax, s[k], Bm[k], um[k], db[k], hod[k]);
+    }
+    V3<R> hv[2] = {hod[0], hod[1]};
+    if (HODP) ldf_pair(a.Hpre, idx, hv[0], hv[1]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int ii[3] = {ix + k, iy, iz};
+      if (!PER) stage_sat<R, SoA<R>, HALL>(a, ii, nn, idx + k, Bm[k], um[k], CONV, db[k]);
+      if (HOD_) {
+        db[k].x += a.hod_factor * hv[k].x;
+        db[k].y += a.hod_factor * hv[k].y;
+        db[k].z += a.hod_factor * hv[k].z;
+      }
+      if (FOAD) {
+        const V3<R> ds = fo_ad_dissipation<R, SoA<R>, OP, PER>(a, ii, nn, st, idx + k, Bm[k], um[k]);
+        db[k].x += ds.x; db[k].y += ds.y; db[k].z += ds.z;
       }
     }
     stage_epilogue_pair(a, idx, db[0], db[1]);

@@ -24,6 +24,7 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
 TOL64 = 1e-12
 TOL32 = 2e-5
 TWO_PI_ = 2.0 * math.pi
+HP_ = 4.0 * math.pi / 3.0   # period of the hall_periodic testcase
 
 
 def _golden():
@@ -502,7 +503,8 @@ def test_column_block_shape_does_not_change_the_result(shape, case):
     assert np.isfinite(out[0]).all() and np.abs(out[0]).max() > 0
 
 
-@pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32"])
+@pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32", "periodic_conv_hod",
+                                  "periodic_fo", "periodic_adaptive_conv"])
 def test_two_nodes_per_thread_equal_one_node_per_thread(case):
     # the Hall column kernels with two x-adjacent nodes per thread form every node's sums in
     # the order of the one-node kernels: the fields agree up to the compiler's choice of
@@ -517,12 +519,19 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
         c.update(real="float")
     if case.startswith("box"):
         c.update(testcase="hall_travelling_wave")
+    if "conv" in case:   # variable velocity: the convection sums beside the Hall term
+        c.update(testcase="hall_periodic", hi=HP_, variable_u=True, dt=1e-3)
+    if case.endswith("fo"):
+        c.update(dissipation="FIRST_ORDER")
+    if case.startswith("periodic_adaptive"):
+        c.update(dissipation="ADAPTIVE")
     out = []
     for pairs in (0, 1):
         ctx = maps_for(dict(c, col_pairs=pairs)).context()
         dev = [ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
                ctx.scalar(np.zeros(2), n=2)]
         ctx.kernel("init_b", dev[0])
+        ctx.kernel("init_u", dev[4])
         ctx.time_steps(*dev, 3)
         out.append([ctx.get_vec(dev[0]), ctx.get_vec(dev[1]), ctx.get_vec(dev[3])])
     scale = float(np.abs(out[0][0]).max())
