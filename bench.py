@@ -642,6 +642,33 @@ def main() -> None:
                     roofline["traffic_note"] = ("ncu capture with caches flushed before the launch: the inputs "
                                                 "come from DRAM, the writes stay in L2")
 
+    # the FP64 roof beside the HBM roof: the device's FMA-loop rate (measured here, after the
+    # timed region) and the stage kernel's FP64 FLOPs per launch (2 x DFMA + DADD + DMUL
+    # thread instructions from an ncu count, in the kernel's summary under profiles/)
+    flops = None
+    if os.path.isfile(summary):
+        with open(summary) as f:
+            for line in f:
+                if line.startswith("fp64_flops_per_launch:"):
+                    flops = int(line.split(":", 1)[1].strip())
+    from inductioneq_b200 import lib as L
+    fp64_peak_tflops = L.fp64_fma_rate(dev) / 1e3
+    fp64_roof = {"bound": "fp64", "peak": fp64_peak_tflops, "unit": "TFLOP/s",
+                 "peak_source": "measured: ieq_fp64_fma_rate (FMA loop, 8 chains per thread, 8 blocks of 256 per SM)"}
+    if flops:
+        fp64_roof.update({"achieved": flops / stage_avg / 1e12, "frac": flops / stage_avg / 1e12 / fp64_peak_tflops,
+                          "flops_per_launch": flops, "flops_per_node": flops / nn,
+                          "flops_source": "ncu thread-instruction counts: 2 x DFMA + DADD + DMUL"})
+    curl_summary = os.path.join(ROOT, "profiles", "k_curl_e_x2_hall6_64cubed.md")
+    if not a.no_pairs and a.stage_kernel != "BRICK" and os.path.isfile(curl_summary):
+        with open(curl_summary) as f:
+            for line in f:
+                if line.startswith("fp64_flops_per_launch:"):
+                    cf = int(line.split(":", 1)[1].strip())
+                    fp64_roof.update({"curl_kernel_flops_per_node": cf / nn,
+                                      "curl_kernel_frac": cf / curl_avg / 1e12 / fp64_peak_tflops})
+    roofline["fp64_roof"] = fp64_roof
+
     out = {
         "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
         "ms_per_step": t_max / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -242,6 +242,12 @@ ieq_status ieq_adjoint_steps(ieq_ctx *ctx, const void *b0, void *lambda, const v
 ieq_status ieq_dot_product_noalloc(const double *a, const double *b, uint64_t n, double *result,
                                    void *stream);
 
+/* The FP64 arithmetic rate of `device` in GFLOP/s (2 per fused multiply-add), measured with
+ * an FMA loop of `iterations` steps per chain (8 independent chains per thread, 8 blocks of
+ * 256 threads per SM) timed with CUDA events: the FP64 roof the stencil kernels are graded
+ * against beside the HBM bandwidth.  No counterpart in the reference (a measurement aid). */
+ieq_status ieq_fp64_fma_rate(int device, int iterations, double *gflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,7 @@ def load() -> ctypes.CDLL:
     lib.ieq_adjoint_steps.argtypes = [vp] * 5 + [ctypes.c_int, ctypes.c_int]
     lib.ieq_status_string.argtypes = [ctypes.c_int]
     lib.ieq_status_string.restype = ctypes.c_char_p
+    lib.ieq_fp64_fma_rate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     _LIB = lib
     return lib
 
@@ -308,3 +309,13 @@ class Context:
 
     def check_finite(self, b) -> None:
         self._check(self.lib.ieq_check_finite(self.h, _ptr(b)))
+
+
+def fp64_fma_rate(device: int = 0, iterations: int = 20000) -> float:
+    """The device's FP64 rate in GFLOP/s, measured with an FMA loop (ieq_fp64_fma_rate)."""
+    lib = load()
+    g = ctypes.c_double(0.0)
+    st = lib.ieq_fp64_fma_rate(int(device), int(iterations), ctypes.byref(g))
+    if st != 0:
+        raise IeqError(st, lib.ieq_status_string(st).decode())
+    return g.value
