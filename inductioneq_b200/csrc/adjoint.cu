@@ -484,6 +484,27 @@ ieq_status ieq_ssprk33_step_vjp(ieq_ctx *c, const void *s1, const void *s2, cons
 // Adjoint of num_steps SSPRK33 steps from b0 (time 0): lambda holds dL/db(T) on entry and
 // dL/db0 on return.  The forward run is checkpointed every `checkpoint_every` steps; each
 // segment is recomputed (stage states kept) and swept backwards.
+}  // extern "C"
+
+namespace {
+// n zeroed vector fields from the context's adjoint pool (grown on demand, kept until
+// ieq_destroy, so repeated sweeps allocate nothing)
+ieq_status adj_pool(ieq_ctx *c, size_t n, size_t bytes, std::vector<void *> &out) {
+  while (c->adj_bufs.size() < n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return afail(c, IEQ_ERR_CUDA, "adjoint work allocation");
+    c->adj_bufs.push_back(p);
+  }
+  if (!c->adj_time && cudaMalloc(&c->adj_time, 4 * sizeof(double)) != cudaSuccess)
+    return afail(c, IEQ_ERR_CUDA, "adjoint work allocation");
+  out.assign(c->adj_bufs.begin(), c->adj_bufs.begin() + (long)n);
+  for (void *p : out) cudaMemsetAsync(p, 0, bytes, c->stream);
+  return IEQ_OK;
+}
+}  // namespace
+
+extern "C" {
+
 ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const void *u, const void *rho, int num_steps,
                              int checkpoint_every) {
   if (!c || !b0 || !lambda || !u || !rho || num_steps < 0 || checkpoint_every < 1) return IEQ_ERR_ARG;
@@ -494,19 +515,16 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   const size_t vb = c->n_pad * sizeof(R4<double>);
   const int K = checkpoint_every;
   const int nseg = (num_steps + K - 1) / K;
-  std::vector<void *> ck, seg, w;
+  // checkpoints (nseg), the stage states of one segment (3K), step work (5), step-adjoint work (7)
+  std::vector<void *> pool;
+  if ((st = adj_pool(c, (size_t)nseg + 3 * K + 12, vb, pool)) != IEQ_OK) return st;
+  std::vector<void *> ck(pool.begin(), pool.begin() + nseg), seg(pool.begin() + nseg, pool.begin() + nseg + 3 * K),
+      w(pool.begin() + nseg + 3 * K, pool.begin() + nseg + 3 * K + 5);
   VjpWork vw;
-  if ((st = work_alloc(c, ck, nseg, vb)) != IEQ_OK || (st = work_alloc(c, seg, 3 * K, vb)) != IEQ_OK ||
-      (st = work_alloc(c, w, 5, vb)) != IEQ_OK || (st = vjp_work_alloc(c, vw)) != IEQ_OK) {
-    free_all(ck);
-    free_all(seg);
-    free_all(w);
-    vjp_work_free(vw);
-    return st;
-  }
+  vw.f.assign(pool.begin() + nseg + 3 * K + 5, pool.end());
+  vw.d_time = c->adj_time + 2;
   void *cur = w[0], *b2 = w[1], *b3 = w[2], *cb = w[3], *uw = w[4];
-  double *d_time = nullptr;
-  cudaMalloc(&d_time, 2 * sizeof(double));
+  double *d_time = c->adj_time;
   std::vector<double> t0s(num_steps + 1, 0.0);
   for (int n = 0; n < num_steps; ++n) t0s[n + 1] = t0s[n] + c->s.dt;   // calc_time_3_args
   auto step = [&](void *state, double t0, void *keep1, void *keep2, void *keep3) -> ieq_status {
@@ -546,11 +564,6 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
                                rho, vw);
   }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "adjoint sweep");
-  cudaFree(d_time);
-  free_all(ck);
-  free_all(seg);
-  free_all(w);
-  vjp_work_free(vw);
   return st;
 }
 

@@ -221,10 +221,11 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
 
 // the block shape of a column kernel (x, y, z threads; all zero: the default) and whether
 // the Hall kernels run two nodes per thread
-static ColShape col_shape(const int (&b)[3], bool pairs) {
+static ColShape col_shape(const int (&b)[3], bool pairs, bool pdl) {
   ColShape sh;
   if (b[0] > 0) sh = ColShape{b[0], b[1], b[2]};
   sh.pairs = pairs;
+  sh.pdl = pdl;
   return sh;
 }
 
@@ -232,7 +233,7 @@ template <typename R>
 void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, bool hodp = false) {
   const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
   const bool foad = diss_kind(c->s) == DISS_FO_OR_AD;
-  const ColShape sh = col_shape(c->s.col_block, c->s.col_pairs);
+  const ColShape sh = col_shape(c->s.col_block, c->s.col_pairs, c->s.pdl);
   switch (c->op_id) {
     case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
     case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
@@ -263,7 +264,7 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
         a.Hint[s + i + RI] += (((R)op.minv[op.nb] * (R)op.DHO.at(op.nb, s + WH - 1)) * (R)op.DHO.at(op.nb, i)) * sgn;
   }
   const bool per = c->s.periodic;
-  const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs);
+  const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs, c->s.pdl);
   switch (c->op_id) {
     case 0: launch_curl_e<R, 0>(a, per, hod, sh, c->stream); break;
     case 1: launch_curl_e<R, 1>(a, per, hod, sh, c->stream); break;
@@ -810,6 +811,8 @@ void ieq_destroy(ieq_ctx *c) {
     if (kv.second.exec2) cudaGraphExecDestroy(kv.second.exec2);
   }
   for (void *p : c->allocs) cudaFree(p);
+  for (void *p : c->adj_bufs) cudaFree(p);
+  if (c->adj_time) cudaFree(c->adj_time);
   void *own[] = {c->d_tables, c->d_rows_r, c->d_rows_d, c->d_lap_r, c->d_lap_d, c->d_wnorm, c->d_partials,
                  c->d_partials2, c->d_total, c->d_counter, c->d_flag, c->d_cg, c->d_cg_vec, c->d_cg_hist,
                  c->d_pingpong, c->d_soa};

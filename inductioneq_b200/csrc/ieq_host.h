@@ -49,6 +49,8 @@ struct Settings {
   // IEQ_COL_PAIRS=0: the Hall column kernels keep one node per thread (default 1: two
   // x-adjacent nodes per thread where nx and the field layout allow it)
   bool col_pairs = true;
+  // IEQ_PDL=0: launch the Hall pair kernels without programmatic dependent launch
+  bool pdl = true;
 };
 
 // parse helpers (settings.cpp)
@@ -98,6 +100,8 @@ struct ieq_ctx {
   int cg_hist_len = 0;
   void *d_pingpong = nullptr;      // (unused)
   void *d_soa = nullptr;           // structure-of-arrays state of the fused time stepping
+  std::vector<void *> adj_bufs;    // vector fields of the checkpointed adjoint, kept for later calls
+  double *adj_time = nullptr;      // its two time pairs
   void *brick_maps = nullptr;      // tensor maps of that state for the TMA brick kernels (host)
   std::set<void *> allocs;
   // fused time-step graphs keyed by the argument pointers

@@ -135,6 +135,12 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         err = key + " must be XxYxZ with X * Y * Z = 128 (e.g. 32x4x1)";
         return false;
       }
+    } else if (key == "IEQ_PDL") {
+      if (val != "0" && val != "1") {
+        err = "IEQ_PDL must be 0 or 1";
+        return false;
+      }
+      s.pdl = val == "1";
     } else if (key == "IEQ_COL_PAIRS") {
       if (val != "0" && val != "1") {
         err = "IEQ_COL_PAIRS must be 0 or 1";

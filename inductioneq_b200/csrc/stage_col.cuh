@@ -47,6 +47,33 @@ __device__ __forceinline__ R cmp(const V3<R> &v, int ax) {
   return ax == 0 ? v.x : (ax == 1 ? v.y : v.z);
 }
 
+// Programmatic dependent launch: the curl and stage kernels of consecutive stages depend on
+// each other's complete output.  Launched with programmatic stream serialization (launch_pdl), a kernel may be scheduled while its predecessor still runs; each block first
+// waits for the predecessor grid to complete and its writes to be visible (griddepcontrol.wait,
+// a hardware dependency wait that ends when the predecessor ends) and only then allows its own
+// dependents to be scheduled (griddepcontrol.launch_dependents).  No block reads or writes
+// fields before its wait, and a kernel never runs more than one launch ahead.  Launched
+// without the attribute both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename Kern, typename Arg>
+inline void launch_pdl(Kern kernel, dim3 grid, dim3 block, cudaStream_t s, bool pdl, const Arg &a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <typename R>
 struct ColSums {
   V3<R> SuiBa, SU, SB, SuaB, SHo;
@@ -174,6 +201,7 @@ template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, int NEED
           bool FOAD = false>
 __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS : IEQ_COL_MIN_BLOCKS) * 128 / kColThreads) k_stage_col(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, RI = Op<OP>::RI;
+  pdl_enter();
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
   const int need = NEED >= 0 ? NEED : a.need;
   constexpr int NZ = col_nodes(CONV);
@@ -293,6 +321,7 @@ __global__ void __launch_bounds__(kColThreads, (CONV ? IEQ_COL_CONV_MIN_BLOCKS :
 template <typename R, int OP, bool PER>
 __global__ void __launch_bounds__(kColThreads) k_curl_e(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
+  pdl_enter();
   constexpr int NZ = kCurlNodes;
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -477,6 +506,7 @@ __device__ __forceinline__ void curl_axis_node(const CurlArgs<R, SoA<R>> &a, int
 template <typename R, int OP, bool PER>
 __global__ void __launch_bounds__(kColThreads, IEQ_CURL_MIN_BLOCKS * 128 / kColThreads)
     k_curl_e_hod(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+  pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -538,6 +568,7 @@ __global__ void k_soa_ssp104_06(long long n, SoA<R> b1, SoA<R> b2, SoA<R> b3, R 
 struct ColShape {
   int x = 32, y = 4, z = 1;
   bool pairs = true;
+  bool pdl = true;   // programmatic dependent launch of the pair kernels (stage_x2.cuh)
 };
 inline dim3 col_block(ColShape sh) { return dim3((unsigned)sh.x, (unsigned)sh.y, (unsigned)sh.z); }
 inline dim3 col_grid(ColShape sh, int nx, int ny, int nz, int nodes) {

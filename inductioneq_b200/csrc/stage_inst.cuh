@@ -65,40 +65,40 @@ void launch_curl<IEQ_R, SoA<IEQ_R>, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a
 // the column kernels of the fused path (no first-order / adaptive dissipation)
 template <bool P, bool H>
 static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
-                          dim3 b, cudaStream_t s) {
+                          dim3 b, bool pdl, cudaStream_t s) {
   // (a flux-form mask compiled in for the default forms measured 3-10 % slower for orders
   // 4 and 6 on B200: the mask stays a run-time value)
   if (foad) {
-    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1, -1, false, true><<<g, b, 0, s>>>(a);
-    else k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0, -1, false, true><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1, -1, false, true>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0, -1, false, true>, g, b, s, pdl, a);
   } else if (hod && hodp) {
-    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1, -1, true><<<g, b, 0, s>>>(a);
-    else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0, -1, true><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1, -1, true>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0, -1, true>, g, b, s, pdl, a);
   } else if (hod) {
-    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1><<<g, b, 0, s>>>(a);
-    else k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, true, 1>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, true, 0>, g, b, s, pdl, a);
   } else {
-    if (conv) k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1><<<g, b, 0, s>>>(a);
-    else k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, false, 1>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col<IEQ_R, IEQ_OP, P, H, false, 0>, g, b, s, pdl, a);
   }
 }
 
 // the same with two x-adjacent nodes per thread (k_stage_col_x2)
 template <bool P, bool H>
 static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
-                             dim3 b, cudaStream_t s) {
+                             dim3 b, bool pdl, cudaStream_t s) {
   if (foad) {
-    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1, false, true><<<g, b, 0, s>>>(a);
-    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0, false, true><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1, false, true>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0, false, true>, g, b, s, pdl, a);
   } else if (hod && hodp) {
-    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1, true><<<g, b, 0, s>>>(a);
-    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0, true><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1, true>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0, true>, g, b, s, pdl, a);
   } else if (hod) {
-    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1><<<g, b, 0, s>>>(a);
-    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0>, g, b, s, pdl, a);
   } else {
-    if (conv) k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1><<<g, b, 0, s>>>(a);
-    else k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0><<<g, b, 0, s>>>(a);
+    if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1>, g, b, s, pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0>, g, b, s, pdl, a);
   }
 }
 
@@ -113,11 +113,11 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
       pair_ok(a.out3)) {
     const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
     if (per) {
-      if (hodp) k_stage_hall_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
-      else k_stage_hall_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true>, g2, b, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, false>, g2, b, s, sh.pdl, a);
     } else {
-      if (hodp) k_stage_hall_x2<IEQ_R, IEQ_OP, false, true><<<g2, b, 0, s>>>(a);
-      else k_stage_hall_x2<IEQ_R, IEQ_OP, false, false><<<g2, b, 0, s>>>(a);
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true>, g2, b, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false>, g2, b, s, sh.pdl, a);
     }
     return;
   }
@@ -129,15 +129,16 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && per && hall && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1), b, s);
+    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1), b, sh.pdl,
+                                 s);
     return;
   }
   if (per) {
-    if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, foad, g, b, s);
-    else launch_col_ph<true, false>(a, hod, conv, false, foad, g, b, s);
+    if (hall) launch_col_ph<true, true>(a, hod, conv, hodp, foad, g, b, sh.pdl, s);
+    else launch_col_ph<true, false>(a, hod, conv, false, foad, g, b, sh.pdl, s);
   } else {
-    if (hall) launch_col_ph<false, true>(a, hod, conv, hodp, foad, g, b, s);
-    else launch_col_ph<false, false>(a, hod, conv, false, foad, g, b, s);
+    if (hall) launch_col_ph<false, true>(a, hod, conv, hodp, foad, g, b, sh.pdl, s);
+    else launch_col_ph<false, false>(a, hod, conv, false, foad, g, b, sh.pdl, s);
   }
 }
 
@@ -150,19 +151,19 @@ void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per
   if (sh.pairs && per && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
       (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
     const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
-    if (hod) k_curl_e_x2<IEQ_R, IEQ_OP, true, true><<<g2, b, 0, s>>>(a);
-    else k_curl_e_x2<IEQ_R, IEQ_OP, true, false><<<g2, b, 0, s>>>(a);
+    if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true>, g2, b, s, sh.pdl, a);
+    else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false>, g2, b, s, sh.pdl, a);
     return;
   }
   if (hod) {
     const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, 1);
-    if (per) k_curl_e_hod<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
-    else k_curl_e_hod<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
+    if (per) launch_pdl(k_curl_e_hod<IEQ_R, IEQ_OP, true>, g, b, s, sh.pdl, a);
+    else launch_pdl(k_curl_e_hod<IEQ_R, IEQ_OP, false>, g, b, s, sh.pdl, a);
     return;
   }
   const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
-  if (per) k_curl_e<IEQ_R, IEQ_OP, true><<<g, b, 0, s>>>(a);
-  else k_curl_e<IEQ_R, IEQ_OP, false><<<g, b, 0, s>>>(a);
+  if (per) launch_pdl(k_curl_e<IEQ_R, IEQ_OP, true>, g, b, s, sh.pdl, a);
+  else launch_pdl(k_curl_e<IEQ_R, IEQ_OP, false>, g, b, s, sh.pdl, a);
 }
 
 // the TMA brick kernels (u = 0 stages); the dynamic shared memory limit of each

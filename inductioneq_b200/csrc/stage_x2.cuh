@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
   constexpr int QL = (RI + 1) / 2;
+  pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -338,6 +339,7 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
     k_stage_hall_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
   constexpr int QL = (RI + 1) / 2;
+  pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -555,6 +557,7 @@ template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HOD
 __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS)
     k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
+  pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;

@@ -111,6 +111,8 @@ class Maps:
                 s += f" -D{name}=" + "x".join(str(int(v)) for v in self.I_Tech[key])
         if self.I_Tech.get("col_pairs") is not None:   # Hall column kernels: two nodes per thread
             s += f" -DIEQ_COL_PAIRS={int(bool(self.I_Tech['col_pairs']))}"
+        if self.I_Tech.get("pdl") is not None:   # programmatic dependent launch of the pair kernels
+            s += f" -DIEQ_PDL={int(bool(self.I_Tech['pdl']))}"
         return s
 
     def kernel_path_list(self) -> list[str]:

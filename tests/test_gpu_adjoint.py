@@ -177,3 +177,34 @@ def test_checkpointed_gradient_matches_central_differences_via_autograd():
         assert e3 <= 0.05 * e1 or e3 <= 1e-9 * abs(ad), (k, e1, e3)
         rich = (4.0 * f2 - f1) / 3.0
         assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
+
+
+def test_repeated_sweeps_on_one_context_reuse_the_checkpoint_pool():
+    # the checkpointed sweep keeps its work fields in the context: later calls with other
+    # step counts and checkpoint spacings (smaller and larger pools) give the gradients of
+    # a fresh context
+    ctx, dt = _c5_small()
+    b = ctx.vec()
+    ctx.kernel("init_b", b)
+    u = ctx.vec()
+    ctx.kernel("init_u", u)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    seed = np.random.default_rng(7).standard_normal((ctx.n_pad, 4))
+    seed[:, 3] = 0
+    seed[ctx.n:] = 0
+
+    def grad(c, nsteps, every):
+        lam = c.vec(seed)
+        c.adjoint_steps(b if c is ctx else c.vec(ctx.get_vec(b)), lam, u if c is ctx else c.vec(ctx.get_vec(u)),
+                        rho if c is ctx else c.scalar(np.ones(c.n_pad)), nsteps, every)
+        return c.get_vec(lam)
+
+    plans = [(6, 3), (12, 5), (4, 4), (6, 3)]
+    got = [grad(ctx, *p) for p in plans]
+    for p, g in zip(plans, got):
+        fresh, _ = _c5_small()
+        ref = grad(fresh, *p)
+        fresh.close()
+        assert np.array_equal(g, ref), p
+    assert np.array_equal(got[0], got[3])
+    ctx.close()
