@@ -568,8 +568,21 @@ __global__ void k_soa_ssp104_06(long long n, SoA<R> b1, SoA<R> b2, SoA<R> b3, R 
 struct ColShape {
   int x = 32, y = 4, z = 1;
   bool pairs = true;
-  bool pdl = true;   // programmatic dependent launch of the pair kernels (stage_x2.cuh)
+  bool pdl = true;     // programmatic dependent launch of the column kernels
+  bool given = false;  // the shape was set explicitly (else the kernels' defaults apply)
 };
+// the default shape of the pair kernels, measured on B200 (Hall whistler, 6th order + HOD):
+// the curl kernel 32 x 2 x 2 (64^3: 6.24 us against 6.46 for 32 x 4 x 1; 128^3: equal); the
+// stage kernel 32 x 2 x 2 while the fields stay L2 resident (<= 2^20 nodes; 64^3: 7.20
+// against 7.32 us) and 32 x 4 x 1 above (128^3: 53.1 against 53.7 us)
+inline ColShape pair_shape(ColShape sh, bool curl, long long nodes) {
+  if (!sh.given && (curl || nodes <= (1ll << 20))) {
+    sh.x = 32;
+    sh.y = 2;
+    sh.z = 2;
+  }
+  return sh;
+}
 inline dim3 col_block(ColShape sh) { return dim3((unsigned)sh.x, (unsigned)sh.y, (unsigned)sh.z); }
 inline dim3 col_grid(ColShape sh, int nx, int ny, int nz, int nodes) {
   const int zb = sh.z * nodes;

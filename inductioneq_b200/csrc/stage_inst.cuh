@@ -111,13 +111,14 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && hall && !conv && !foad && (hodp || !hod) && a.m.nx % 2 == 0 && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz);
+    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (per) {
-      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true>, g2, b, s, sh.pdl, a);
-      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, false>, g2, b, s, sh.pdl, a);
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, false>, g2, b2, s, sh.pdl, a);
     } else {
-      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true>, g2, b, s, sh.pdl, a);
-      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false>, g2, b, s, sh.pdl, a);
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true>, g2, b2, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false>, g2, b2, s, sh.pdl, a);
     }
     return;
   }
@@ -129,8 +130,9 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && per && hall && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1), b, sh.pdl,
-                                 s);
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz);
+    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), col_block(ps),
+                                 sh.pdl, s);
     return;
   }
   if (per) {
@@ -150,9 +152,10 @@ void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per
   // one-node kernels measured faster)
   if (sh.pairs && per && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
       (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
-    const dim3 g2 = col_grid(sh, a.m.nx / 2, a.m.ny, a.m.nz, 1);
-    if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true>, g2, b, s, sh.pdl, a);
-    else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false>, g2, b, s, sh.pdl, a);
+    const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz);
+    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
+    if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);
+    else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false>, g2, b2, s, sh.pdl, a);
     return;
   }
   if (hod) {
