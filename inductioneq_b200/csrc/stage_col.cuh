@@ -575,13 +575,26 @@ struct ColShape {
 // the curl kernel 32 x 2 x 2 (64^3: 6.24 us against 6.46 for 32 x 4 x 1; 128^3: equal); the
 // stage kernel 32 x 2 x 2 while the fields stay L2 resident (<= 2^20 nodes; 64^3: 7.20
 // against 7.32 us) and 32 x 4 x 1 above (128^3: 53.1 against 53.7 us)
-inline ColShape pair_shape(ColShape sh, bool curl, long long nodes) {
+// Rows that are not a multiple of 32 threads long (nxe = nodes, or node pairs, per x row)
+// get a block x extent that divides them evenly: ceil(nxe / ceil(nxe / 32)) threads, the
+// other dimensions refilled towards 128 threads (a 16-node row as 32 threads would leave
+// half the lanes idle; the batched form's small grids are of this kind).
+inline ColShape fit_rows(ColShape sh, int nxe) {
+  if (sh.given || nxe % 32 == 0) return sh;
+  const int nbx = (nxe + 31) / 32;
+  sh.x = (nxe + nbx - 1) / nbx;
+  const int yz = kColThreads / sh.x;
+  sh.z = sh.z > 1 && yz >= 2 ? 2 : 1;
+  sh.y = yz / sh.z > 0 ? yz / sh.z : 1;
+  return sh;
+}
+inline ColShape pair_shape(ColShape sh, bool curl, long long nodes, int nx) {
   if (!sh.given && (curl || nodes <= (1ll << 20))) {
     sh.x = 32;
     sh.y = 2;
     sh.z = 2;
   }
-  return sh;
+  return fit_rows(sh, nx / 2);
 }
 inline dim3 col_block(ColShape sh) { return dim3((unsigned)sh.x, (unsigned)sh.y, (unsigned)sh.z); }
 inline dim3 col_grid(ColShape sh, int nx, int ny, int nz, int nodes) {

@@ -105,13 +105,14 @@ static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, in
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
                                      bool hodp, bool foad, ColShape sh, cudaStream_t s) {
-  const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block(sh);
+  const ColShape s1 = fit_rows(sh, a.m.nx);
+  const dim3 g = col_grid(s1, a.m.nx, a.m.ny, a.m.nz, col_nodes(conv)), b = col_block(s1);
   // the precomputed dissipation sum comes with the Hall curl kernel only
   hodp = hodp && hall && hod && !foad;
   if (sh.pairs && hall && !conv && !foad && (hodp || !hod) && a.m.nx % 2 == 0 && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz);
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (per) {
       if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);
@@ -130,9 +131,22 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && per && hall && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz);
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), col_block(ps),
                                  sh.pdl, s);
+    return;
+  }
+  // convection without the Hall term, with the reference's default flux forms (product
+  // u_i B_j, central source and u_j B_i: the sums D[u] and D[u_a B_i] only, fixed at compile
+  // time, which keeps two nodes' sums in 128 registers): measured 2-10 % faster than one node
+  // per thread (rotation, orders 2/4/6, 64^3 .. 128^3); other forms keep one node per thread
+  if (sh.pairs && !hall && conv && !hod && !foad && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
+      pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
+      pair_ok(a.out3)) {
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
+    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
+    if (per) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, false, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
     return;
   }
   if (per) {
@@ -147,24 +161,25 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
 template <>
 void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hod, ColShape sh,
                                   cudaStream_t s) {
-  const dim3 b = col_block(sh);
+  const ColShape s1 = fit_rows(sh, a.m.nx);
+  const dim3 b = col_block(s1);
   // pairs on periodic grids only (on boxes the x boundary rows run per node and the
   // one-node kernels measured faster)
   if (sh.pairs && per && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
       (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
-    const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz);
+    const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);
     else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false>, g2, b2, s, sh.pdl, a);
     return;
   }
   if (hod) {
-    const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, 1);
+    const dim3 g = col_grid(s1, a.m.nx, a.m.ny, a.m.nz, 1);
     if (per) launch_pdl(k_curl_e_hod<IEQ_R, IEQ_OP, true>, g, b, s, sh.pdl, a);
     else launch_pdl(k_curl_e_hod<IEQ_R, IEQ_OP, false>, g, b, s, sh.pdl, a);
     return;
   }
-  const dim3 g = col_grid(sh, a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
+  const dim3 g = col_grid(s1, a.m.nx, a.m.ny, a.m.nz, kCurlNodes);
   if (per) launch_pdl(k_curl_e<IEQ_R, IEQ_OP, true>, g, b, s, sh.pdl, a);
   else launch_pdl(k_curl_e<IEQ_R, IEQ_OP, false>, g, b, s, sh.pdl, a);
 }

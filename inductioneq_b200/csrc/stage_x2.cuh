@@ -463,11 +463,11 @@ __device__ __forceinline__ void col_load_pair(const StageArgs<R, SoA<R>> &a, int
 }
 
 // the x sums of the pair (ix, ix + 1) on the interior row (or with periodic wrap)
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
 __device__ __forceinline__ void col_x_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, long long row0, int ix,
                                            int nx) {
   constexpr int RI = Op<OP>::RI, QL = (RI + 1) / 2;
-  const int need = a.need;
+  const int need = NEED >= 0 ? NEED : a.need;
   const V3<R> zero = {0, 0, 0};
 #pragma unroll
   for (int q = -QL; q <= QL; ++q) {
@@ -498,12 +498,12 @@ __device__ __forceinline__ void col_x_pair(ColSums<R> (&s)[2], const StageArgs<R
 }
 
 // the y or z sums of the pair (both nodes on the same row of the axis)
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV>
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
 __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, int ax, int i, int n,
                                             long long idx, long long st, const V3<R> (&Bm)[2]) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
-  const int need = a.need;
+  const int need = NEED >= 0 ? NEED : a.need;
   const V3<R> zero = {0, 0, 0};
   const int row = PER ? NB : sbp_row(i, n, NB);
   if (row == NB) {
@@ -553,7 +553,8 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
 // DB (volume, Hall, SAT, dissipation) and the stage update at the pair; template
 // arguments as k_stage_col (CONV = 1: the convection sums; HODP: the dissipation sum read
 // from a.Hpre; FOAD: first-order / adaptive dissipation)
-template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false>
+template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false,
+          int NEED = -1>
 __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS)
     k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
@@ -572,11 +573,11 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
     {
       ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
       if (x_pair_interior<OP, PER>(ix, nx)) {
-        col_x_pair<R, OP, PER, HALL, HOD, CONV>(s, a, row0, ix, nx);
+        col_x_pair<R, OP, PER, HALL, HOD, CONV, NEED>(s, a, row0, ix, nx);
       } else {
 #pragma unroll
         for (int k = 0; k < 2; ++k)
-          col_axis<R, OP, PER, HALL, HOD, CONV>(s[k], a, 0, ix + k, nx, idx + k, 1, Bm[k]);
+          col_axis<R, OP, PER, HALL, HOD, CONV, SoA<R>, NEED>(s[k], a, 0, ix + k, nx, idx + k, 1, Bm[k]);
       }
 #pragma unroll
       for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, 0, s[k], Bm[k], um[k], db[k], hod[k]);
@@ -586,7 +587,7 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
 #pragma unroll
     for (int ax = 1; ax < 3; ++ax) {
       ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
-      col_yz_pair<R, OP, PER, HALL, HOD, CONV>(s, a, ax, ax == 1 ? iy : iz, nn[ax], idx, st[ax], Bm);
+      col_yz_pair<R, OP, PER, HALL, HOD, CONV, NEED>(s, a, ax, ax == 1 ? iy : iz, nn[ax], idx, st[ax], Bm);
 #pragma unroll
       for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, ax, s[k], Bm[k], um[k], db[k], hod[k]);
     }
