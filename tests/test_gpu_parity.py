@@ -232,6 +232,49 @@ def test_fused_column_kernel_cases(name):
     np.testing.assert_allclose(ctx.get_scalar(dev[6], n=2), host[6], rtol=1e-15 if o.T == np.float64 else 1e-6)
 
 
+# Hall + convection (the testcase's velocity) through the pair kernels with the flux-form
+# mask fixed at compile time: a box (x boundary pairs per node, SAT) and a periodic grid with
+# the dissipation sum precomputed; nx even so that the pair kernels run
+HALL_CONV_CASES = {
+    "confined_4c_hall_conv_box": dict(order=4, testcase="confined_domain", nodes=(16, 13, 14), lo=0.0, hi=1.0,
+                                      hall=True, integrator="CarpenterKennedy2N54", dt=1e-5, steps=2),
+    "hallper_6c_hall_conv_hod_per": dict(order=6, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0, hi=HP_,
+                                         periodic=True, hall=True, dissipation="HIGH_ORDER", integrator="SSPRK33",
+                                         dt=1e-3, steps=2),
+    "confined_2c_hall_conv_box_f32": dict(order=2, testcase="confined_domain", nodes=(14, 12, 10), lo=0.0, hi=1.0,
+                                          hall=True, integrator="SSPRK33", dt=1e-5, steps=2, real="float"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(HALL_CONV_CASES))
+def test_fused_hall_convection_pairs_match_oracle(name):
+    c = HALL_CONV_CASES[name]
+    ctx = maps_for(c).context()
+    o = oracle_for(c)
+    b, uf = ctx.vec(), ctx.vec()
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", uf)
+    u = ctx.get_vec(uf).astype(o.T)
+    assert np.abs(u).max() > 0           # the convection terms are present
+    bh = ctx.get_vec(b).astype(np.float64)
+    bh[: ctx.n, :3] += 1e-2 * np.random.default_rng(NOISE_SEED).standard_normal((ctx.n, 3))
+    bh = bh.astype(o.T)
+    nf = NUM_FIELDS[c["integrator"]]
+    host = [bh.copy(), np.zeros_like(bh), np.zeros_like(bh), np.zeros_like(bh), u, np.ones(o.N, dtype=o.T),
+            np.zeros(2, dtype=o.T)]
+    dev = [ctx.vec(host[0]), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(u), ctx.scalar(host[5]),
+           ctx.scalar(host[6], n=2)]
+    time_loop(o, c["integrator"], True, False, c["steps"], host[0], host[1], host[2] if nf == 3 else None,
+              host[3], host[4], host[5], host[6])
+    ctx.time_steps(*dev, c["steps"])
+    scale = float(np.abs(host[0]).max())
+    for i in (0, 1, 3):
+        got = ctx.get_vec(dev[i])
+        e = float(np.abs(got - host[i]).max()) / (scale if i == 1 else float(np.abs(host[i]).max()))
+        assert e <= tol(c), (i, e)
+    assert rel_err(host[0], bh) > 1e-7
+
+
 @pytest.mark.parametrize("name", ["wave_6c_hall_hod_ck2n54", "rot_gauss_4c_ssprk33"])
 def test_fused_time_steps_are_bitwise_reproducible(name):
     z, _ = _golden()
