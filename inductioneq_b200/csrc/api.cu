@@ -222,13 +222,14 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
 // the block shape of a column kernel (x, y, z threads, from IEQ_COL_BLOCK / IEQ_CURL_BLOCK;
 // all zero: the kernels' defaults, see pair_shape) and whether the Hall kernels run two
 // nodes per thread
-static ColShape col_shape(const int (&b)[3], bool pairs, bool pdl) {
+static ColShape col_shape(const int (&b)[3], int pairs, bool pdl) {
   ColShape sh;
   if (b[0] > 0) {
     sh = ColShape{b[0], b[1], b[2]};
     sh.given = true;
   }
-  sh.pairs = pairs;
+  sh.pairs = pairs != 0;
+  sh.quads = pairs == 4;
   sh.pdl = pdl;
   return sh;
 }

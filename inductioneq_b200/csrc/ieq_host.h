@@ -46,9 +46,10 @@ struct Settings {
   // kernel (IEQ_CURL_BLOCK); X * Y * Z = 128, all zero for the default 32x4x1
   int col_block[3] = {0, 0, 0};
   int curl_block[3] = {0, 0, 0};
-  // IEQ_COL_PAIRS=0: the Hall column kernels keep one node per thread (default 1: two
-  // x-adjacent nodes per thread where nx and the field layout allow it)
-  bool col_pairs = true;
+  // IEQ_COL_PAIRS=0: the column kernels keep one node per thread; 1 (default): two
+  // x-adjacent nodes per thread where measured faster and the field layout allows it (FP32
+  // Hall kernels: four on grids of >= 2^20 nodes); 4: FP32 Hall kernels four on every grid
+  int col_pairs = 1;
   // IEQ_PDL=0: launch the Hall pair kernels without programmatic dependent launch
   bool pdl = true;
 };

@@ -142,11 +142,11 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
       }
       s.pdl = val == "1";
     } else if (key == "IEQ_COL_PAIRS") {
-      if (val != "0" && val != "1") {
-        err = "IEQ_COL_PAIRS must be 0 or 1";
+      if (val != "0" && val != "1" && val != "4") {
+        err = "IEQ_COL_PAIRS must be 0, 1 or 4";
         return false;
       }
-      s.col_pairs = val == "1";
+      s.col_pairs = std::atoi(val.c_str());
     } else if (key == "USE_HALL") {
       s.hall = true;
     } else if (key == "USE_PERIODIC") {

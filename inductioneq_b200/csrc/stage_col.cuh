@@ -570,6 +570,7 @@ struct ColShape {
   bool pairs = true;
   bool pdl = true;     // programmatic dependent launch of the column kernels
   bool given = false;  // the shape was set explicitly (else the kernels' defaults apply)
+  bool quads = false;  // FP32 Hall kernels: four nodes per thread on every grid that allows it
 };
 // the default shape of the pair kernels, measured on B200 (Hall whistler, 6th order + HOD):
 // the curl kernel 32 x 2 x 2 (64^3: 6.24 us against 6.46 for 32 x 4 x 1; 128^3: equal); the
@@ -588,13 +589,13 @@ inline ColShape fit_rows(ColShape sh, int nxe) {
   sh.y = yz / sh.z > 0 ? yz / sh.z : 1;
   return sh;
 }
-inline ColShape pair_shape(ColShape sh, bool curl, long long nodes, int nx) {
+inline ColShape pair_shape(ColShape sh, bool curl, long long nodes, int nx, int K = 2) {
   if (!sh.given && (curl || nodes <= (1ll << 20))) {
     sh.x = 32;
     sh.y = 2;
     sh.z = 2;
   }
-  return fit_rows(sh, nx / 2);
+  return fit_rows(sh, nx / K);
 }
 inline dim3 col_block(ColShape sh) { return dim3((unsigned)sh.x, (unsigned)sh.y, (unsigned)sh.z); }
 inline dim3 col_grid(ColShape sh, int nx, int ny, int nz, int nodes) {

@@ -83,6 +83,25 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
   }
 }
 
+// the Hall stage kernel without convection, K x-adjacent nodes per thread
+template <int K>
+static void launch_stage_hall_k(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hodp, ColShape sh,
+                                cudaStream_t s) {
+  if constexpr (K == 4 && sizeof(IEQ_R) != 4) {
+    return;   // (quads are FP32 only; the caller never asks for them in FP64)
+  } else {
+    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx, K);
+    const dim3 g = col_grid(ps, a.m.nx / K, a.m.ny, a.m.nz, 1), b = col_block(ps);
+    if (per) {
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true, K>, g, b, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, false, K>, g, b, s, sh.pdl, a);
+    } else {
+      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true, K>, g, b, s, sh.pdl, a);
+      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false, K>, g, b, s, sh.pdl, a);
+    }
+  }
+}
+
 // the same with two x-adjacent nodes per thread (k_stage_col_x2)
 template <bool P, bool H>
 static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
@@ -112,15 +131,14 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && hall && !conv && !foad && (hodp || !hod) && a.m.nx % 2 == 0 && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
-    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
-    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
-    if (per) {
-      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);
-      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, true, false>, g2, b2, s, sh.pdl, a);
-    } else {
-      if (hodp) launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true>, g2, b2, s, sh.pdl, a);
-      else launch_pdl(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false>, g2, b2, s, sh.pdl, a);
+    // FP32: four nodes per thread (float4) where the fields allow it
+    if (sizeof(IEQ_R) == 4 && (sh.quads || quads_fill((long long)a.m.nx * a.m.ny * a.m.nz)) && a.m.nx % 4 == 0 &&
+        group_ok<4>(a.E) && group_ok<4>(a.Hpre) && group_ok<4>(a.X) &&
+        group_ok<4>(a.Y) && group_ok<4>(a.Z) && group_ok<4>(a.out) && group_ok<4>(a.out2) && group_ok<4>(a.out3)) {
+      launch_stage_hall_k<4>(a, per, hodp, sh, s);
+      return;
     }
+    launch_stage_hall_k<2>(a, per, hodp, sh, s);
     return;
   }
   // Hall + convection with the default flux forms (the two convection sums per axis fixed
@@ -185,6 +203,18 @@ void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per
   // one-node kernels measured faster)
   if (sh.pairs && per && a.m.nx % 2 == 0 && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
       (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
+    if constexpr (sizeof(IEQ_R) == 4) {
+      // FP32: four nodes per thread (float4) where the fields allow it
+      if ((sh.quads || quads_fill((long long)a.m.nx * a.m.ny * a.m.nz)) && a.m.nx % 4 == 0 && group_ok<4>(a.b) &&
+          group_ok<4>(a.out) && group_ok<4>(a.hout) &&
+          (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % 16 == 0)) {
+        const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx, 4);
+        const dim3 g4 = col_grid(ps, a.m.nx / 4, a.m.ny, a.m.nz, 1), b4 = col_block(ps);
+        if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true, 4>, g4, b4, s, sh.pdl, a);
+        else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false, 4>, g4, b4, s, sh.pdl, a);
+        return;
+      }
+    }
     const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (hod) launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, true>, g2, b2, s, sh.pdl, a);

@@ -76,19 +76,98 @@ __device__ __forceinline__ R &cref(V3<R> &v, int c) {
   return c == 0 ? v.x : (c == 1 ? v.y : v.z);
 }
 
-// the x window of one component for the pair at (row0 + ix, row0 + ix + 1):
-// w[m] = f[row0 + ix - 2QL + m], m = 0 .. 4QL+1, periodic wrap of the pair starts
-template <typename R, int QL, bool PER>
-__device__ __forceinline__ void x_window(const R *f, long long row0, int ix, int nx, R (&w)[4 * QL + 2]) {
+// K consecutive values (K = 2: FP64 or FP32 pairs; K = 4: FP32 quads) in one vector load
+template <typename R, int K>
+struct VecK;
+template <>
+struct VecK<double, 2> {
+  using T = double2;
+};
+template <>
+struct VecK<float, 2> {
+  using T = float2;
+};
+template <>
+struct VecK<float, 4> {
+  using T = float4;
+};
+template <typename R, int K>
+__device__ __forceinline__ void unpack_k(const typename VecK<R, K>::T &v, R (&o)[K]) {
+  o[0] = v.x;
+  o[1] = v.y;
+  if constexpr (K == 4) {
+    o[2] = v.z;
+    o[3] = v.w;
+  }
+}
+// the values at j .. j + K - 1 (j a multiple of K) through the read-only path
+template <typename R, int K>
+__device__ __forceinline__ void ld_k(const R *p, R (&o)[K]) {
+  unpack_k<R, K>(__ldg(reinterpret_cast<const typename VecK<R, K>::T *>(p)), o);
+}
+template <typename R, int K>
+__device__ __forceinline__ void ld_k_plain(const R *p, R (&o)[K]) {
+  unpack_k<R, K>(*reinterpret_cast<const typename VecK<R, K>::T *>(p), o);
+}
+template <typename R, int K>
+__device__ __forceinline__ void st_k(R *p, const R (&o)[K]) {
+  typename VecK<R, K>::T v;
+  v.x = o[0];
+  v.y = o[1];
+  if constexpr (K == 4) {
+    v.z = o[2];
+    v.w = o[3];
+  }
+  *reinterpret_cast<typename VecK<R, K>::T *>(p) = v;
+}
+template <typename R, int K, bool PLAIN = false>
+__device__ __forceinline__ void ldf_k(const SoA<R> &f, long long j, V3<R> (&a)[K]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    R t[K];
+    if (PLAIN) ld_k_plain<R, K>(f.p + j + c * f.s, t);
+    else ld_k<R, K>(f.p + j + c * f.s, t);
+#pragma unroll
+    for (int k = 0; k < K; ++k) cref(a[k], c) = t[k];
+  }
+}
+template <typename R, int K>
+__device__ __forceinline__ void stf_k(const SoA<R> &f, long long j, const V3<R> (&a)[K]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    R t[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) t[k] = cmp(a[k], c);
+    st_k<R, K>(f.p + j + c * f.s, t);
+  }
+}
+
+// the x window of one component for the K nodes row0 + ix .. row0 + ix + K - 1:
+// w[m] = f[row0 + ix - K*QL + m], m = 0 .. K*(2QL+1) - 1, periodic wrap of the group starts
+template <typename R, int K, int QL, bool PER>
+__device__ __forceinline__ void x_window_k(const R *f, long long row0, int ix, int nx, R (&w)[K * (2 * QL + 1)]) {
 #pragma unroll
   for (int q = -QL; q <= QL; ++q) {
-    int xx = ix + 2 * q;
+    int xx = ix + K * q;
     if (PER) {
       xx += xx < 0 ? nx : 0;
       xx -= xx >= nx ? nx : 0;
     }
-    ld_pair(f + row0 + xx, w[2 * (q + QL)], w[2 * (q + QL) + 1]);
+    R t[K];
+    ld_k<R, K>(f + row0 + xx, t);
+#pragma unroll
+    for (int k = 0; k < K; ++k) w[K * (q + QL) + k] = t[k];
   }
+}
+
+// whether the group's x stencils may use the window (all K nodes on the interior row and
+// the window inside the row; always with periodic wrap)
+template <int OP, bool PER, int K>
+__device__ __forceinline__ bool x_group_interior(int ix, int nx) {
+  constexpr int NB = Op<OP>::NB, QL = (Op<OP>::RI + K - 1) / K;
+  if (PER) return true;
+  return sbp_row(ix, nx, NB) == NB && sbp_row(ix + K - 1, nx, NB) == NB && ix - K * QL >= 0 &&
+         ix + K * QL + K - 1 < nx;
 }
 
 // whether the pair's x stencils may use the window (both nodes on the interior row and
@@ -114,17 +193,31 @@ __device__ __forceinline__ bool x_pair_interior(int ix, int nx) {
 #ifndef IEQ_STAGE_X2_MIN_BLOCKS
 #define IEQ_STAGE_X2_MIN_BLOCKS 7
 #endif
+// FP32 with four nodes per thread (float4 loads; measured at 128^3: curl 4 blocks of <= 128
+// registers, stage 7 blocks of <= 72: 22.9 / 29.5 us against 29.0 / 35.3 with pairs)
+#ifndef IEQ_CURL_X4_MIN_BLOCKS
+#define IEQ_CURL_X4_MIN_BLOCKS 4
+#endif
+#ifndef IEQ_STAGE_X4_MIN_BLOCKS
+#define IEQ_STAGE_X4_MIN_BLOCKS 7
+#endif
 
-// J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at the pair of nodes
-template <typename R, int OP, bool PER, bool HODS>
-__global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : IEQ_CURL_X2_PLAIN_MIN_BLOCKS)
+// whether FP32 runs four nodes per thread: only where a quarter of the nodes still fills
+// the GPU (>= 2^20 nodes; at 64^3 the quads leave about 14 warps per SM and measured slower
+// than pairs)
+inline bool quads_fill(long long nodes) { return nodes >= (1ll << 20); }
+
+// J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at K x-adjacent nodes
+template <typename R, int OP, bool PER, bool HODS, int K = 2>
+__global__ void __launch_bounds__(kColThreads, HODS ? (K == 4 ? IEQ_CURL_X4_MIN_BLOCKS : IEQ_CURL_X2_MIN_BLOCKS)
+                                                   : IEQ_CURL_X2_PLAIN_MIN_BLOCKS)
     k_curl_e_x2(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
-  constexpr int QL = (RI + 1) / 2;
+  constexpr int QL = (RI + K - 1) / K;
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int ix = K * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
   if (ix >= nx || iy >= ny || iz >= nz) return;
@@ -132,18 +225,20 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
   const long long idx = row0 + ix;
   const long long cs = a.b.s;
   const V3<R> zero = {0, 0, 0};
-  V3<R> Bm[2];
-  ldf_pair(a.b, idx, Bm[0], Bm[1]);
-  R g[2][3][3];
-  V3<R> hod[2] = {zero, zero};
+  V3<R> Bm[K];
+  ldf_k<R, K>(a.b, idx, Bm);
+  R g[K][3][3];
+  V3<R> hod[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) hod[k] = zero;
 
   // x
   {
-    R v1[2], v2[2];
-    V3<R> ho[2];
-    if (x_pair_interior<OP, PER>(ix, nx)) {
+    R v1[K], v2[K];
+    V3<R> ho[K];
+    if (x_group_interior<OP, PER, K>(ix, nx)) {
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
+      for (int k = 0; k < K; ++k) {
         v1[k] = 0;
         v2[k] = 0;
         ho[k] = zero;
@@ -151,13 +246,13 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if (!HODS && c == 0) continue;   // the x derivatives of By and Bz only
-        R w[4 * QL + 2];
-        x_window<R, QL, PER>(a.b.p + c * cs, row0, ix, nx, w);
+        R w[K * (2 * QL + 1)];
+        x_window_k<R, K, QL, PER>(a.b.p + c * cs, row0, ix, nx, w);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < K; ++k) {
 #pragma unroll
           for (int o = -RI; o <= RI; ++o) {
-            const R val = w[2 * QL + k + o];
+            const R val = w[K * QL + k + o];
             if (o != 0) {
               if (c == 1) v1[k] += a.Dint[o + RI] * val;
               if (c == 2) v2[k] += a.Dint[o + RI] * val;
@@ -168,11 +263,11 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
       }
     } else {
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
+      for (int k = 0; k < K; ++k)
         curl_axis_node<R, OP, PER, HODS>(a, 0, ix + k, nx, idx + k, 1, Bm[k], v1[k], v2[k], ho[k]);
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < K; ++k) {
       g[k][0][1] = v1[k] * a.inv_d[0];
       g[k][0][2] = v2[k] * a.inv_d[0];
       if (HODS) {
@@ -181,7 +276,7 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
     }
   }
 
-  // y and z: both nodes on the same row of the axis
+  // y and z: all K nodes on the same row of the axis
   const int ii[3] = {ix, iy, iz};
   const int nn[3] = {nx, ny, nz};
   const long long st[3] = {1, nx, (long long)nx * ny};
@@ -189,8 +284,14 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
   for (int ax = 1; ax < 3; ++ax) {
     const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
     const int i = ii[ax], n = nn[ax];
-    R v1[2] = {0, 0}, v2[2] = {0, 0};
-    V3<R> ho[2] = {zero, zero};
+    R v1[K], v2[K];
+    V3<R> ho[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      v1[k] = 0;
+      v2[k] = 0;
+      ho[k] = zero;
+    }
     const int row = PER ? NB : sbp_row(i, n, NB);
     if (row == NB) {
       const bool wrap = PER && (i < RI || i >= n - RI);
@@ -200,7 +301,7 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
         if (o == 0) {
           if (HODS) {
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
+            for (int k = 0; k < K; ++k) {
               ho[k].x += cH * Bm[k].x; ho[k].y += cH * Bm[k].y; ho[k].z += cH * Bm[k].z;
             }
           }
@@ -209,20 +310,20 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
         const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
         const R c = a.Dint[o + RI];
         if (HODS) {
-          V3<R> B[2];
-          ldf_pair(a.b, j, B[0], B[1]);
+          V3<R> B[K];
+          ldf_k<R, K>(a.b, j, B);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             v1[k] += c * cmp(B[k], c1);
             v2[k] += c * cmp(B[k], c2);
             ho[k].x += cH * B[k].x; ho[k].y += cH * B[k].y; ho[k].z += cH * B[k].z;
           }
         } else {
-          R p1[2], p2[2];
-          ld_pair(a.b.p + j + c1 * cs, p1[0], p1[1]);
-          ld_pair(a.b.p + j + c2 * cs, p2[0], p2[1]);
+          R p1[K], p2[K];
+          ld_k<R, K>(a.b.p + j + c1 * cs, p1);
+          ld_k<R, K>(a.b.p + j + c2 * cs, p2);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             v1[k] += c * p1[k];
             v2[k] += c * p2[k];
           }
@@ -235,10 +336,10 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
         if (cD == (R)0 && cH == (R)0) continue;
         const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
         if (HODS) {
-          V3<R> B[2];
-          ldf_pair(a.b, j, B[0], B[1]);
+          V3<R> B[K];
+          ldf_k<R, K>(a.b, j, B);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             if (cD != (R)0) {
               v1[k] += cD * cmp(B[k], c1);
               v2[k] += cD * cmp(B[k], c2);
@@ -248,11 +349,11 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
             }
           }
         } else {
-          R p1[2], p2[2];
-          ld_pair(a.b.p + j + c1 * cs, p1[0], p1[1]);
-          ld_pair(a.b.p + j + c2 * cs, p2[0], p2[1]);
+          R p1[K], p2[K];
+          ld_k<R, K>(a.b.p + j + c1 * cs, p1);
+          ld_k<R, K>(a.b.p + j + c2 * cs, p2);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             v1[k] += cD * p1[k];
             v2[k] += cD * p2[k];
           }
@@ -260,7 +361,7 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
       }
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < K; ++k) {
       g[k][ax][c1] = v1[k] * a.inv_d[ax];
       g[k][ax][c2] = v2[k] * a.inv_d[ax];
       if (HODS) {
@@ -269,11 +370,11 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
     }
   }
 
-  R r[2] = {1, 1};
-  if (a.rho) ld_pair(a.rho + idx, r[0], r[1]);
-  V3<R> E[2];
+  R r[K];
+  if (a.rho) ld_k<R, K>(a.rho + idx, r);
+  V3<R> E[K];
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < K; ++k) {
     V3<R> J = {g[k][1][2] - g[k][2][1], g[k][2][0] - g[k][0][2], g[k][0][1] - g[k][1][0]};
     if (a.rho) {
       const R ri = (R)1 / r[k];
@@ -284,64 +385,79 @@ __global__ void __launch_bounds__(kColThreads, HODS ? IEQ_CURL_X2_MIN_BLOCKS : I
     if (!PER && (ix + k == 0 || iy == 0 || iz == 0 || ix + k == nx - 1 || iy == ny - 1 || iz == nz - 1))
       stf(a.jface, idx + k, J);
   }
-  stf_pair(a.out, idx, E[0], E[1]);
-  if (HODS) stf_pair(a.hout, idx, hod[0], hod[1]);
+  stf_k<R, K>(a.out, idx, E);
+  if (HODS) stf_k<R, K>(a.hout, idx, hod);
 }
 
-// the stage update of the pair from DB (epilogue modes of stage_kernel.cuh), with pair loads
+// the stage update of K nodes from DB (epilogue modes of stage_kernel.cuh), with vector loads
 // and stores of the fields it combines
-template <typename R>
-__device__ __forceinline__ void epilogue_load_pair(const StageArgs<R, SoA<R>> &a, long long idx, EpIn<R> (&e)[2]) {
+template <typename R, int K>
+__device__ __forceinline__ void epilogue_load_k(const StageArgs<R, SoA<R>> &a, long long idx, EpIn<R> (&e)[K]) {
   const V3<R> zero = {0, 0, 0};
-  e[0] = EpIn<R>{zero, zero};
-  e[1] = e[0];
+  V3<R> x[K], y[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) x[k] = y[k] = zero;
   switch (a.mode) {
     case EP_X_PLUS_HF:
     case EP_AX_HF:
     case EP_2R_FUSED:
-      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
+      ldf_k<R, K, true>(a.X, idx, x);
       break;
     case EP_PX_QYHF:
-      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
-      ldf_pair_plain(a.Y, idx, e[0].Y, e[1].Y);
+      ldf_k<R, K, true>(a.X, idx, x);
+      ldf_k<R, K, true>(a.Y, idx, y);
       break;
     case EP_2N_FUSED:
-      ldf_pair_plain(a.X, idx, e[0].X, e[1].X);
-      ldf_pair_plain(a.Z, idx, e[0].Y, e[1].Y);
+      ldf_k<R, K, true>(a.X, idx, x);
+      ldf_k<R, K, true>(a.Z, idx, y);
       break;
     case EP_2N_FUSED_FIRST:
-      ldf_pair_plain(a.Z, idx, e[0].Y, e[1].Y);
+      ldf_k<R, K, true>(a.Z, idx, y);
       break;
     default:
       break;
   }
+#pragma unroll
+  for (int k = 0; k < K; ++k) e[k] = EpIn<R>{x[k], y[k]};
 }
-template <typename R>
-__device__ __forceinline__ void epilogue_store_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
-                                                    const V3<R> &d1, const EpIn<R> (&e)[2]) {
-  const EpOut<R> o0 = epilogue_values(a, d0, e[0]), o1 = epilogue_values(a, d1, e[1]);
-  stf_pair(a.out, idx, o0.o1, o1.o1);
-  if (epilogue_writes_out2(a.mode)) stf_pair(a.out2, idx, o0.o2, o1.o2);
-  if (a.mode == EP_2R_FUSED && a.out3.p) stf_pair(a.out3, idx, o0.o3, o1.o3);
+template <typename R, int K>
+__device__ __forceinline__ void epilogue_store_k(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> (&d)[K],
+                                                 const EpIn<R> (&e)[K]) {
+  V3<R> o1[K], o2[K], o3[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const EpOut<R> o = epilogue_values(a, d[k], e[k]);
+    o1[k] = o.o1;
+    o2[k] = o.o2;
+    o3[k] = o.o3;
+  }
+  stf_k<R, K>(a.out, idx, o1);
+  if (epilogue_writes_out2(a.mode)) stf_k<R, K>(a.out2, idx, o2);
+  if (a.mode == EP_2R_FUSED && a.out3.p) stf_k<R, K>(a.out3, idx, o3);
+}
+template <typename R, int K>
+__device__ __forceinline__ void stage_epilogue_k(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> (&d)[K]) {
+  EpIn<R> e[K];
+  epilogue_load_k<R, K>(a, idx, e);
+  epilogue_store_k<R, K>(a, idx, d, e);
 }
 template <typename R>
 __device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &a, long long idx, const V3<R> &d0,
                                                     const V3<R> &d1) {
-  EpIn<R> e[2];
-  epilogue_load_pair(a, idx, e);
-  epilogue_store_pair(a, idx, d0, d1, e);
+  const V3<R> d[2] = {d0, d1};
+  stage_epilogue_k<R, 2>(a, idx, d);
 }
 
-// DB of a Hall stage without convection terms at the pair, with the dissipation sum
-// precomputed (HODP, read from a.Hpre) or absent, and the stage update
-template <typename R, int OP, bool PER, bool HODP>
-__global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
+// DB of a Hall stage without convection terms at K x-adjacent nodes, with the dissipation
+// sum precomputed (HODP, read from a.Hpre) or absent, and the stage update
+template <typename R, int OP, bool PER, bool HODP, int K = 2>
+__global__ void __launch_bounds__(kColThreads, K == 4 ? IEQ_STAGE_X4_MIN_BLOCKS : IEQ_STAGE_X2_MIN_BLOCKS)
     k_stage_hall_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
-  constexpr int QL = (RI + 1) / 2;
+  constexpr int QL = (RI + K - 1) / K;
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int ix = K * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
   if (ix < nx && iy < ny && iz < nz) {
@@ -349,33 +465,37 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
     const long long idx = row0 + ix;
     const long long es = a.E.s;
     const V3<R> zero = {0, 0, 0};
-    V3<R> db[2] = {zero, zero};
+    V3<R> db[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) db[k] = zero;
 
     // x: DB_y += D[Exy], DB_z += D[Exz]
     {
-      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
-      if (x_pair_interior<OP, PER>(ix, nx)) {
+      ColSums<R> s[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) s[k] = ColSums<R>{};
+      if (x_group_interior<OP, PER, K>(ix, nx)) {
 #pragma unroll
         for (int ci = 0; ci < 2; ++ci) {
-          R w[4 * QL + 2];
-          x_window<R, QL, PER>(a.E.p + (ci == 0 ? e_comp1(0) : e_comp2(0)) * es, row0, ix, nx, w);
+          R w[K * (2 * QL + 1)];
+          x_window_k<R, K, QL, PER>(a.E.p + (ci == 0 ? e_comp1(0) : e_comp2(0)) * es, row0, ix, nx, w);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
 #pragma unroll
             for (int o = -RI; o <= RI; ++o) {
               if (o == 0) continue;
-              if (ci == 0) s[k].h1 += a.Dint[o + RI] * w[2 * QL + k + o];
-              else s[k].h2 += a.Dint[o + RI] * w[2 * QL + k + o];
+              if (ci == 0) s[k].h1 += a.Dint[o + RI] * w[K * QL + k + o];
+              else s[k].h2 += a.Dint[o + RI] * w[K * QL + k + o];
             }
           }
         }
       } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < K; ++k)
           col_axis<R, OP, PER, true, false, 0>(s[k], a, 0, ix + k, nx, idx + k, 1, zero);
       }
 #pragma unroll
-      for (int k = 0; k < 2; ++k) col_combine<R, true, false, 0>(a, 0, s[k], zero, zero, db[k], db[k]);
+      for (int k = 0; k < K; ++k) col_combine<R, true, false, 0>(a, 0, s[k], zero, zero, db[k], db[k]);
     }
 
     // y and z
@@ -386,7 +506,9 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
     for (int ax = 1; ax < 3; ++ax) {
       const int i = ii[ax], n = nn[ax];
       const R *e1p = a.E.p + e_comp1(ax) * es, *e2p = a.E.p + e_comp2(ax) * es;
-      ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
+      ColSums<R> s[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) s[k] = ColSums<R>{};
       const int row = PER ? NB : sbp_row(i, n, NB);
       if (row == NB) {
         const bool wrap = PER && (i < RI || i >= n - RI);
@@ -394,12 +516,12 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
         for (int o = -RI; o <= RI; ++o) {
           if (o == 0) continue;
           const long long j = wrap ? idx + (long long)(nbr<true>(i, o, n) - i) * st[ax] : idx + (long long)o * st[ax];
-          R p1[2], p2[2];
-          ld_pair(e1p + j, p1[0], p1[1]);
-          ld_pair(e2p + j, p2[0], p2[1]);
+          R p1[K], p2[K];
+          ld_k<R, K>(e1p + j, p1);
+          ld_k<R, K>(e2p + j, p2);
           const R c = a.Dint[o + RI];
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             s[k].h1 += c * p1[k];
             s[k].h2 += c * p2[k];
           }
@@ -409,24 +531,26 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
           const R cD = a.tab->D[row][o + C0];
           if (cD == (R)0) continue;
           const long long j = idx + (long long)(nbr<PER>(i, o, n) - i) * st[ax];
-          R p1[2], p2[2];
-          ld_pair(e1p + j, p1[0], p1[1]);
-          ld_pair(e2p + j, p2[0], p2[1]);
+          R p1[K], p2[K];
+          ld_k<R, K>(e1p + j, p1);
+          ld_k<R, K>(e2p + j, p2);
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
+          for (int k = 0; k < K; ++k) {
             s[k].h1 += cD * p1[k];
             s[k].h2 += cD * p2[k];
           }
         }
       }
 #pragma unroll
-      for (int k = 0; k < 2; ++k) col_combine<R, true, false, 0>(a, ax, s[k], zero, zero, db[k], db[k]);
+      for (int k = 0; k < K; ++k) col_combine<R, true, false, 0>(a, ax, s[k], zero, zero, db[k], db[k]);
     }
 
-    V3<R> hv[2] = {zero, zero};
-    if (HODP) ldf_pair(a.Hpre, idx, hv[0], hv[1]);
+    V3<R> hv[K];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < K; ++k) hv[k] = zero;
+    if (HODP) ldf_k<R, K>(a.Hpre, idx, hv);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
       if (!PER) {
         const int iik[3] = {ix + k, iy, iz};
         stage_sat<R, SoA<R>, true>(a, iik, nn, idx + k, ldf(a.bk, idx + k), zero, 0, db[k]);
@@ -437,7 +561,7 @@ __global__ void __launch_bounds__(kColThreads, IEQ_STAGE_X2_MIN_BLOCKS)
         db[k].z += a.hod_factor * hv[k].z;
       }
     }
-    stage_epilogue_pair(a, idx, db[0], db[1]);
+    stage_epilogue_k<R, K>(a, idx, db);
   }
   stage_time_post(a);
 }
@@ -610,6 +734,12 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
     stage_epilogue_pair(a, idx, db[0], db[1]);
   }
   stage_time_post(a);
+}
+
+// whether every K-wide load or store of a field is aligned (K elements, stride a multiple of K)
+template <int K, typename R>
+inline bool group_ok(const SoA<R> &f) {
+  return f.p == nullptr || ((reinterpret_cast<uintptr_t>(f.p) % (K * sizeof(R))) == 0 && f.s % K == 0);
 }
 
 // whether a launch may use the pair kernels: nx even and every pair load or store aligned

@@ -109,8 +109,8 @@ class Maps:
         for key, name in (("col_block", "IEQ_COL_BLOCK"), ("curl_block", "IEQ_CURL_BLOCK")):
             if self.I_Tech.get(key):   # (x, y, z) threads of that column kernel, x * y * z = 128
                 s += f" -D{name}=" + "x".join(str(int(v)) for v in self.I_Tech[key])
-        if self.I_Tech.get("col_pairs") is not None:   # Hall column kernels: two nodes per thread
-            s += f" -DIEQ_COL_PAIRS={int(bool(self.I_Tech['col_pairs']))}"
+        if self.I_Tech.get("col_pairs") is not None:   # nodes per thread of the column kernels: 0, 1, 4
+            s += f" -DIEQ_COL_PAIRS={int(self.I_Tech['col_pairs'])}"
         if self.I_Tech.get("pdl") is not None:   # programmatic dependent launch of the pair kernels
             s += f" -DIEQ_PDL={int(bool(self.I_Tech['pdl']))}"
         return s

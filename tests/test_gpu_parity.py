@@ -548,7 +548,8 @@ def test_column_block_shape_does_not_change_the_result(shape, case):
 
 @pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32", "periodic_conv_hod",
                                   "periodic_fo", "periodic_adaptive_conv", "rotation_o2", "rotation_o4",
-                                  "rotation_o6_f32"])
+                                  "rotation_o6_f32", "quads_periodic_hod_f32", "quads_box_hod_f32",
+                                  "quads_periodic_plain_f32"])
 def test_two_nodes_per_thread_equal_one_node_per_thread(case):
     # the Hall column kernels with two x-adjacent nodes per thread form every node's sums in
     # the order of the one-node kernels: the fields agree up to the compiler's choice of
@@ -569,11 +570,19 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
         c.update(dissipation="FIRST_ORDER")
     if case.startswith("periodic_adaptive"):
         c.update(dissipation="ADAPTIVE")
+    if case.startswith("quads"):      # FP32 Hall kernels with four nodes per thread (float4)
+        c.update(real="float", nodes=(16, 12, 14) if "periodic" in case else (20, 13, 14))
+        if "periodic" in case:
+            c.update(periodic=True)
+        else:
+            c.update(testcase="hall_travelling_wave")
+        if "hod" in case:
+            c.update(dissipation="HIGH_ORDER")
     if case.startswith("rotation"):   # convection only, default flux forms, inflow SAT
         c = dict(order=int(case[10]), testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                  integrator="SSPRK33", dt=0.01, real="float" if case.endswith("f32") else "double")
     out = []
-    for pairs in (0, 1):
+    for pairs in (0, 4 if case.startswith("quads") else 1):
         ctx = maps_for(dict(c, col_pairs=pairs)).context()
         dev = [ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
                ctx.scalar(np.zeros(2), n=2)]
