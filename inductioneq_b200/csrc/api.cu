@@ -222,7 +222,7 @@ void launch_stage_any(ieq_ctx *c, const StageArgs<R, F> &a, int conv = -1) {
 // the block shape of a column kernel (x, y, z threads, from IEQ_COL_BLOCK / IEQ_CURL_BLOCK;
 // all zero: the kernels' defaults, see pair_shape) and whether the Hall kernels run two
 // nodes per thread
-static ColShape col_shape(const int (&b)[3], int pairs, bool pdl) {
+static ColShape col_shape(const int (&b)[3], int pairs, bool pdl, int band) {
   ColShape sh;
   if (b[0] > 0) {
     sh = ColShape{b[0], b[1], b[2]};
@@ -231,6 +231,7 @@ static ColShape col_shape(const int (&b)[3], int pairs, bool pdl) {
   sh.pairs = pairs != 0;
   sh.quads = pairs == 4;
   sh.pdl = pdl;
+  sh.band = band;
   return sh;
 }
 
@@ -238,7 +239,7 @@ template <typename R>
 void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, bool hodp = false) {
   const bool per = c->s.periodic, hall = c->s.hall, hod = diss_kind(c->s) == DISS_HO;
   const bool foad = diss_kind(c->s) == DISS_FO_OR_AD;
-  const ColShape sh = col_shape(c->s.col_block, c->s.col_pairs, c->s.pdl);
+  const ColShape sh = col_shape(c->s.col_block, c->s.col_pairs, c->s.pdl, c->s.xband);
   switch (c->op_id) {
     case 0: launch_stage_col<R, 0>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
     case 1: launch_stage_col<R, 1>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
@@ -269,7 +270,7 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
         a.Hint[s + i + RI] += (((R)op.minv[op.nb] * (R)op.DHO.at(op.nb, s + WH - 1)) * (R)op.DHO.at(op.nb, i)) * sgn;
   }
   const bool per = c->s.periodic;
-  const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs, c->s.pdl);
+  const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs, c->s.pdl, c->s.xband);
   switch (c->op_id) {
     case 0: launch_curl_e<R, 0>(a, per, hod, sh, c->stream); break;
     case 1: launch_curl_e<R, 1>(a, per, hod, sh, c->stream); break;

@@ -50,8 +50,11 @@ struct Settings {
   // x-adjacent nodes per thread where measured faster and the field layout allows it (FP32
   // Hall kernels: four on grids of >= 2^20 nodes); 4: FP32 Hall kernels four on every grid
   int col_pairs = 1;
-  // IEQ_PDL=0: launch the Hall pair kernels without programmatic dependent launch
+  // IEQ_PDL=0: launch the column kernels without programmatic dependent launch
   bool pdl = true;
+  // IEQ_XBAND: boxes run their x boundary columns in a launch of their own -- 0 never, 1
+  // (default) where measured faster (the band at most a tenth of the row), 2 wherever possible
+  int xband = 1;
 };
 
 // parse helpers (settings.cpp)

@@ -135,6 +135,12 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         err = key + " must be XxYxZ with X * Y * Z = 128 (e.g. 32x4x1)";
         return false;
       }
+    } else if (key == "IEQ_XBAND") {
+      if (val != "0" && val != "1" && val != "2") {
+        err = "IEQ_XBAND must be 0, 1 or 2";
+        return false;
+      }
+      s.xband = std::atoi(val.c_str());
     } else if (key == "IEQ_PDL") {
       if (val != "0" && val != "1") {
         err = "IEQ_PDL must be 0 or 1";

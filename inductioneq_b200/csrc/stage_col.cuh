@@ -571,6 +571,8 @@ struct ColShape {
   bool pdl = true;     // programmatic dependent launch of the column kernels
   bool given = false;  // the shape was set explicitly (else the kernels' defaults apply)
   bool quads = false;  // FP32 Hall kernels: four nodes per thread on every grid that allows it
+  int band = 1;        // boxes: x boundary columns in a launch of their own (stage_x2.cuh):
+                       // 0 never, 1 where measured faster, 2 wherever the rows allow
 };
 // the default shape of the pair kernels, measured on B200 (Hall whistler, 6th order + HOD):
 // the curl kernel 32 x 2 x 2 (64^3: 6.24 us against 6.46 for 32 x 4 x 1; 128^3: equal); the

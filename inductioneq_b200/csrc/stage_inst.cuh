@@ -83,6 +83,29 @@ static void launch_col_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int c
   }
 }
 
+// a box's stage as two launches: the pair kernel `kint` over the interior x range
+// [xband, nx - xband) (no time bookkeeping) and the one-node kernel `kband` over the 2 *
+// xband boundary columns of every row (with it)
+template <typename KI, typename KB>
+static void launch_banded(KI kint, KB kband, const StageArgs<IEQ_R, SoA<IEQ_R>> &a, ColShape sh, cudaStream_t s) {
+  constexpr int XB = xband<IEQ_OP>();
+  StageArgs<IEQ_R, SoA<IEQ_R>> ai = a;
+  ai.tpost = TP_NONE;
+  const int np = (a.m.nx - 2 * XB) / 2;
+  const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, 2 * np);
+  launch_pdl(kint, col_grid(ps, np, a.m.ny, a.m.nz, 1), col_block(ps), s, sh.pdl, ai);
+  const long long nb = 2ll * XB * a.m.ny * a.m.nz;
+  launch_pdl(kband, dim3((unsigned)((nb + kColThreads - 1) / kColThreads)), dim3(kColThreads), s, sh.pdl, a);
+}
+// whether a box's stage splits off its x boundary columns: even rows in which the band is at
+// most a tenth of the row (measured on B200: rotation 2nd order 96^3 +10 %, 6th order 128^3
+// +23 %, confined Hall 4th order 128^3 +12 % FP64 / +20 % FP32; 4th order 64^3, a band of
+// 8 of 64 columns, 14 % slower)
+static bool banded(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh) {
+  if (per || sh.band == 0 || a.m.nx % 2 != 0 || a.m.nx < 2 * xband<IEQ_OP>() + 2) return false;
+  return sh.band == 2 || a.m.nx >= 20 * xband<IEQ_OP>();
+}
+
 // the Hall stage kernel without convection, K x-adjacent nodes per thread
 template <int K>
 static void launch_stage_hall_k(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hodp, ColShape sh,
@@ -138,6 +161,15 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
       launch_stage_hall_k<4>(a, per, hodp, sh, s);
       return;
     }
+    if (banded(a, per, sh)) {
+      if (hodp)
+        launch_banded(k_stage_hall_x2<IEQ_R, IEQ_OP, false, true, 2, true>,
+                      k_stage_xband<IEQ_R, IEQ_OP, true, true, 0, -1, true, false>, a, sh, s);
+      else
+        launch_banded(k_stage_hall_x2<IEQ_R, IEQ_OP, false, false, 2, true>,
+                      k_stage_xband<IEQ_R, IEQ_OP, true, false, 0, -1, false, false>, a, sh, s);
+      return;
+    }
     launch_stage_hall_k<2>(a, per, hodp, sh, s);
     return;
   }
@@ -148,6 +180,15 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && hall && conv && !foad && (hodp || !hod) && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
       pair_ok(a.u) && pair_ok(a.E) && pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) &&
       pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
+    if (banded(a, per, sh)) {
+      if (hodp)
+        launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, true, 1, true, false, 10, true>,
+                      k_stage_xband<IEQ_R, IEQ_OP, true, true, 1, 10, true, false>, a, sh, s);
+      else
+        launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, false, 1, false, false, 10, true>,
+                      k_stage_xband<IEQ_R, IEQ_OP, true, false, 1, 10, false, false>, a, sh, s);
+      return;
+    }
     const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (per) {
@@ -179,6 +220,11 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   if (sh.pairs && !hall && conv && !hod && !foad && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
       pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
+    if (banded(a, per, sh)) {
+      launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, 10, true>,
+                    k_stage_xband<IEQ_R, IEQ_OP, false, false, 1, 10, false, false>, a, sh, s);
+      return;
+    }
     const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
     const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
     if (per) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, false, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);

@@ -179,6 +179,18 @@ __device__ __forceinline__ bool x_pair_interior(int ix, int nx) {
   return sbp_row(ix, nx, NB) == NB && sbp_row(ix + 1, nx, NB) == NB && ix - 2 * QL >= 0 && ix + 2 * QL + 1 < nx;
 }
 
+// Boxes: the x boundary columns in a band of their own.  A pair kernel launched with XBAND
+// covers only the nodes xband(OP) <= ix < nx - xband(OP), whose x stencils are all interior
+// rows inside the row (no per-node fallback, no SAT on the x faces in its warps); the 2 *
+// xband(OP) boundary columns of every row run one node per thread in k_stage_xband, which
+// also does the stage's time bookkeeping.  xband is even, >= NUM_BOUNDS and >= the pair
+// window's reach 2*ceil(RI/2).
+template <int OP>
+__host__ __device__ constexpr int xband() {
+  constexpr int nb = Op<OP>::NB + (Op<OP>::NB & 1), w = 2 * ((Op<OP>::RI + 1) / 2);
+  return nb > w ? nb : w;
+}
+
 // resident 128-thread blocks per SM the register allocation targets (measured on B200 at
 // 64^3 and 128^3, FP64: the curl kernel is fastest with 4 blocks of <= 128 registers and
 // no spills, 15-25 % ahead of 5 or 6 blocks with spills; the stage kernel with 7 blocks of
@@ -450,17 +462,18 @@ __device__ __forceinline__ void stage_epilogue_pair(const StageArgs<R, SoA<R>> &
 
 // DB of a Hall stage without convection terms at K x-adjacent nodes, with the dissipation
 // sum precomputed (HODP, read from a.Hpre) or absent, and the stage update
-template <typename R, int OP, bool PER, bool HODP, int K = 2>
+template <typename R, int OP, bool PER, bool HODP, int K = 2, bool XBAND = false>
 __global__ void __launch_bounds__(kColThreads, K == 4 ? IEQ_STAGE_X4_MIN_BLOCKS : IEQ_STAGE_X2_MIN_BLOCKS)
     k_stage_hall_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, RI = Op<OP>::RI;
   constexpr int QL = (RI + K - 1) / K;
+  constexpr int X0 = XBAND ? xband<OP>() : 0;
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const int ix = K * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int ix = X0 + K * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
-  if (ix < nx && iy < ny && iz < nz) {
+  if (ix < nx - X0 && iy < ny && iz < nz) {
     const long long row0 = (long long)nx * (iy + (long long)ny * iz);
     const long long idx = row0 + ix;
     const long long es = a.E.s;
@@ -474,7 +487,7 @@ __global__ void __launch_bounds__(kColThreads, K == 4 ? IEQ_STAGE_X4_MIN_BLOCKS 
       ColSums<R> s[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) s[k] = ColSums<R>{};
-      if (x_group_interior<OP, PER, K>(ix, nx)) {
+      if (XBAND || x_group_interior<OP, PER, K>(ix, nx)) {
 #pragma unroll
         for (int ci = 0; ci < 2; ++ci) {
           R w[K * (2 * QL + 1)];
@@ -678,16 +691,17 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
 // arguments as k_stage_col (CONV = 1: the convection sums; HODP: the dissipation sum read
 // from a.Hpre; FOAD: first-order / adaptive dissipation)
 template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false,
-          int NEED = -1>
+          int NEED = -1, bool XBAND = false>
 __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS)
     k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
+  constexpr int X0 = XBAND ? xband<OP>() : 0;
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int ix = X0 + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
-  if (ix < nx && iy < ny && iz < nz) {
+  if (ix < nx - X0 && iy < ny && iz < nz) {
     const long long row0 = (long long)nx * (iy + (long long)ny * iz);
     const long long idx = row0 + ix;
     const V3<R> zero = {0, 0, 0};
@@ -696,7 +710,7 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
     if (CONV) ldf_pair(a.u, idx, um[0], um[1]);
     {
       ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
-      if (x_pair_interior<OP, PER>(ix, nx)) {
+      if (XBAND || x_pair_interior<OP, PER>(ix, nx)) {
         col_x_pair<R, OP, PER, HALL, HOD, CONV, NEED>(s, a, row0, ix, nx);
       } else {
 #pragma unroll
@@ -732,6 +746,56 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
       }
     }
     stage_epilogue_pair(a, idx, db[0], db[1]);
+  }
+  stage_time_post(a);
+}
+
+// One node of a box's stage in the order of operations of k_stage_col (one node per thread)
+template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD>
+__device__ __forceinline__ void col_stage_node(const StageArgs<R, SoA<R>> &a, int ix, int iy, int iz) {
+  constexpr bool HOD = HOD_ && !HODP;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {nx, ny, nz};
+  const long long st[3] = {1, nx, (long long)nx * ny};
+  const V3<R> zero = {0, 0, 0};
+  const V3<R> Bm = ldf(a.bk, idx);
+  const V3<R> um = CONV ? ldf(a.u, idx) : zero;
+  V3<R> db = zero, hod = zero;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    ColSums<R> s{};
+    col_axis<R, OP, false, HALL, HOD, CONV, SoA<R>, NEED>(s, a, ax, ii[ax], nn[ax], idx, st[ax], Bm);
+    col_combine<R, HALL, HOD, CONV>(a, ax, s, Bm, um, db, hod);
+  }
+  stage_sat<R, SoA<R>, HALL>(a, ii, nn, idx, Bm, um, CONV, db);
+  if (HOD_) {
+    const V3<R> hv = HODP ? ldf(a.Hpre, idx) : hod;
+    db.x += a.hod_factor * hv.x;
+    db.y += a.hod_factor * hv.y;
+    db.z += a.hod_factor * hv.z;
+  }
+  if (FOAD) {
+    const V3<R> ds = fo_ad_dissipation<R, SoA<R>, OP, false>(a, ii, nn, st, idx, Bm, um);
+    db.x += ds.x; db.y += ds.y; db.z += ds.z;
+  }
+  stage_epilogue<R, SoA<R>>(a, idx, db);
+}
+
+// the x boundary columns of a box (2 * xband nodes per row, one per thread), and the stage's
+// time bookkeeping
+template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD>
+__global__ void __launch_bounds__(kColThreads) k_stage_xband(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+  constexpr int XB = xband<OP>();
+  pdl_enter();
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long rows = (long long)a.m.ny * a.m.nz;
+  if (i < rows * 2 * XB) {
+    const int slot = (int)(i % (2 * XB));
+    const long long row = i / (2 * XB);
+    const int ix = slot < XB ? slot : a.m.nx - 2 * XB + slot;
+    col_stage_node<R, OP, HALL, HOD_, CONV, NEED, HODP, FOAD>(a, ix, (int)(row % a.m.ny), (int)(row / a.m.ny));
   }
   stage_time_post(a);
 }

@@ -111,8 +111,10 @@ class Maps:
                 s += f" -D{name}=" + "x".join(str(int(v)) for v in self.I_Tech[key])
         if self.I_Tech.get("col_pairs") is not None:   # nodes per thread of the column kernels: 0, 1, 4
             s += f" -DIEQ_COL_PAIRS={int(self.I_Tech['col_pairs'])}"
-        if self.I_Tech.get("pdl") is not None:   # programmatic dependent launch of the pair kernels
+        if self.I_Tech.get("pdl") is not None:   # programmatic dependent launch of the column kernels
             s += f" -DIEQ_PDL={int(bool(self.I_Tech['pdl']))}"
+        if self.I_Tech.get("xband") is not None:   # boxes: x boundary columns in a launch of their own
+            s += f" -DIEQ_XBAND={int(self.I_Tech['xband'])}"
         return s
 
     def kernel_path_list(self) -> list[str]:

@@ -33,6 +33,7 @@ def maps_for(c: dict) -> Maps:
     m.I_Tech["col_block"] = c.get("col_block")
     m.I_Tech["curl_block"] = c.get("curl_block")
     m.I_Tech["col_pairs"] = c.get("col_pairs")
+    m.I_Tech["xband"] = c.get("xband")
     m.I_RunOps.update({"order": c.get("order", 4), "operator_form": "extended" if c.get("extended") else "classical",
                        "testcase": c["testcase"], "variable_u": c.get("variable_u", False),
                        "periodic": "USE_PERIODIC" if c.get("periodic") else "NONE"})

@@ -596,3 +596,37 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
         e = float(np.abs(a.astype(np.float64) - b).max()) / scale
         assert e <= tol, (i, e)
     assert np.isfinite(out[0][0]).all()
+
+
+@pytest.mark.parametrize("case", ["rotation_o2", "rotation_o6", "hall_box_hod", "hall_box_plain_f32", "hall_conv_box"])
+def test_box_x_band_equals_pair_kernels_alone(case):
+    # boxes run their x boundary columns in a launch of their own (one node per thread) and
+    # the pair kernels over the interior x range: the same sums as the pair kernels with the
+    # boundary columns inside them, up to FMA contraction
+    if case.startswith("rotation"):
+        c = dict(order=int(case[-1]), testcase="rotation_gaussian", nodes=(26, 13, 14), lo=-1.0, hi=1.0,
+                 integrator="SSPRK33", dt=0.01)
+    elif case == "hall_conv_box":
+        c = dict(order=4, testcase="confined_domain", nodes=(18, 13, 14), lo=0.0, hi=1.0, hall=True,
+                 integrator="CarpenterKennedy2N54", dt=1e-5)
+    else:
+        c = dict(order=6, testcase="hall_travelling_wave", nodes=(22, 13, 14), lo=0.0, hi=TWO_PI_, hall=True,
+                 integrator="CarpenterKennedy2N54", dt=0.002, real="float" if case.endswith("f32") else "double")
+        if "hod" in case:
+            c.update(dissipation="HIGH_ORDER")
+    out = []
+    for band in (0, 2):   # never / wherever the rows allow
+        ctx = maps_for(dict(c, xband=band)).context()
+        dev = [ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.kernel("init_b", dev[0])
+        ctx.kernel("init_u", dev[4])
+        ctx.time_steps(*dev, 3)
+        out.append([ctx.get_vec(dev[0]), ctx.get_vec(dev[1]), ctx.get_scalar(dev[6], n=2)])
+    scale = float(np.abs(out[0][0]).max())
+    tol = 2e-6 if c.get("real") == "float" else 1e-13
+    for i in (0, 1):
+        e = float(np.abs(out[0][i].astype(np.float64) - out[1][i]).max()) / scale
+        assert e <= tol, (i, e)
+    np.testing.assert_array_equal(out[0][2], out[1][2])    # time bookkeeping by the band kernel
+    assert np.isfinite(out[1][0]).all()
