@@ -267,6 +267,29 @@ void launch_curl_e<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool per
     else launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, true, false>, g2, b2, s, sh.pdl, a);
     return;
   }
+  // FP32 boxes: the pair kernel over the interior x range and the x boundary columns apart
+  // (the rule of the stage kernels; confined Hall 128^3: 23.7 against 27.0 us).  In FP64 the
+  // one-node kernels stay faster on boxes (128^3: 37.5 / 69 us against 39.2 / 86 us without
+  // / with the dissipation sum), the pair kernel's y and z boundary rows then running at 4
+  // blocks per SM.
+  if (sizeof(IEQ_R) == 4 && !per && sh.pairs && sh.band != 0 && a.m.nx % 2 == 0 && a.m.nx >= 2 * xband<IEQ_OP>() + 2 &&
+      (sh.band == 2 || a.m.nx >= 20 * xband<IEQ_OP>()) && pair_ok(a.b) && pair_ok(a.out) && pair_ok(a.hout) &&
+      (a.rho == nullptr || reinterpret_cast<uintptr_t>(a.rho) % (2 * sizeof(IEQ_R)) == 0)) {
+    constexpr int XB = xband<IEQ_OP>();
+    const int np = (a.m.nx - 2 * XB) / 2;
+    const ColShape ps = pair_shape(sh, true, (long long)a.m.nx * a.m.ny * a.m.nz, 2 * np);
+    const dim3 gi = col_grid(ps, np, a.m.ny, a.m.nz, 1), bi = col_block(ps);
+    const long long nb = 2ll * XB * a.m.ny * a.m.nz;
+    const dim3 gb((unsigned)((nb + kColThreads - 1) / kColThreads)), bb(kColThreads);
+    if (hod) {
+      launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, false, true, 2, true>, gi, bi, s, sh.pdl, a);
+      launch_pdl(k_curl_xband<IEQ_R, IEQ_OP, true>, gb, bb, s, sh.pdl, a);
+    } else {
+      launch_pdl(k_curl_e_x2<IEQ_R, IEQ_OP, false, false, 2, true>, gi, bi, s, sh.pdl, a);
+      launch_pdl(k_curl_xband<IEQ_R, IEQ_OP, false>, gb, bb, s, sh.pdl, a);
+    }
+    return;
+  }
   if (hod) {
     const dim3 g = col_grid(s1, a.m.nx, a.m.ny, a.m.nz, 1);
     if (per) launch_pdl(k_curl_e_hod<IEQ_R, IEQ_OP, true>, g, b, s, sh.pdl, a);

@@ -220,19 +220,20 @@ __host__ __device__ constexpr int xband() {
 inline bool quads_fill(long long nodes) { return nodes >= (1ll << 20); }
 
 // J = curl(B)/rho, E = J x B and (HODS) the dissipation sum H of B at K x-adjacent nodes
-template <typename R, int OP, bool PER, bool HODS, int K = 2>
+template <typename R, int OP, bool PER, bool HODS, int K = 2, bool XBAND = false>
 __global__ void __launch_bounds__(kColThreads, HODS ? (K == 4 ? IEQ_CURL_X4_MIN_BLOCKS : IEQ_CURL_X2_MIN_BLOCKS)
                                                    : IEQ_CURL_X2_PLAIN_MIN_BLOCKS)
     k_curl_e_x2(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = HODS ? ((C0 > WH - 1) ? C0 : WH - 1) : C0;
   constexpr int QL = (RI + K - 1) / K;
+  constexpr int X0 = XBAND ? xband<OP>() : 0;
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
-  const int ix = K * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int ix = X0 + K * (blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
-  if (ix >= nx || iy >= ny || iz >= nz) return;
+  if (ix >= nx - X0 || iy >= ny || iz >= nz) return;
   const long long row0 = (long long)nx * (iy + (long long)ny * iz);
   const long long idx = row0 + ix;
   const long long cs = a.b.s;
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kColThreads, HODS ? (K == 4 ? IEQ_CURL_X4_MIN_
   {
     R v1[K], v2[K];
     V3<R> ho[K];
-    if (x_group_interior<OP, PER, K>(ix, nx)) {
+    if (XBAND || x_group_interior<OP, PER, K>(ix, nx)) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         v1[k] = 0;
@@ -798,6 +799,47 @@ __global__ void __launch_bounds__(kColThreads) k_stage_xband(const __grid_consta
     col_stage_node<R, OP, HALL, HOD_, CONV, NEED, HODP, FOAD>(a, ix, (int)(row % a.m.ny), (int)(row / a.m.ny));
   }
   stage_time_post(a);
+}
+
+// J = curl(B)/rho, E = J x B, (HODS) the dissipation sum and J on the faces at one node of a
+// box's x boundary columns (2 * xband per row, one per thread; the order of k_curl_e_hod)
+template <typename R, int OP, bool HODS>
+__global__ void __launch_bounds__(kColThreads) k_curl_xband(const __grid_constant__ CurlArgs<R, SoA<R>> a) {
+  constexpr int XB = xband<OP>();
+  pdl_enter();
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  if (i >= (long long)ny * nz * 2 * XB) return;
+  const int slot = (int)(i % (2 * XB));
+  const long long row = i / (2 * XB);
+  const int ix = slot < XB ? slot : nx - 2 * XB + slot, iy = (int)(row % ny), iz = (int)(row / ny);
+  const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {nx, ny, nz};
+  const long long st[3] = {1, nx, (long long)nx * ny};
+  const V3<R> Bm = ldf(a.b, idx);
+  R g[3][3];
+  V3<R> hod = {0, 0, 0};
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+    R v1, v2;
+    V3<R> ho;
+    curl_axis_node<R, OP, false, HODS>(a, ax, ii[ax], nn[ax], idx, st[ax], Bm, v1, v2, ho);
+    g[ax][c1] = v1 * a.inv_d[ax];
+    g[ax][c2] = v2 * a.inv_d[ax];
+    if (HODS) {
+      hod.x += ho.x; hod.y += ho.y; hod.z += ho.z;
+    }
+  }
+  V3<R> J = {g[1][2] - g[2][1], g[2][0] - g[0][2], g[0][1] - g[1][0]};
+  if (a.rho) {
+    const R r = (R)1 / a.rho[idx];
+    J = {J.x * r, J.y * r, J.z * r};
+  }
+  stf(a.out, idx, V3<R>{J.x * Bm.y - J.y * Bm.x, J.x * Bm.z - J.z * Bm.x, J.y * Bm.z - J.z * Bm.y});
+  if (HODS) stf(a.hout, idx, hod);
+  if (ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1) stf(a.jface, idx, J);
 }
 
 // whether every K-wide load or store of a field is aligned (K elements, stride a multiple of K)

@@ -598,7 +598,8 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
     assert np.isfinite(out[0][0]).all()
 
 
-@pytest.mark.parametrize("case", ["rotation_o2", "rotation_o6", "hall_box_hod", "hall_box_plain_f32", "hall_conv_box"])
+@pytest.mark.parametrize("case", ["rotation_o2", "rotation_o6", "hall_box_hod", "hall_box_plain_f32", "hall_box_hod_f32",
+                                  "hall_conv_box"])
 def test_box_x_band_equals_pair_kernels_alone(case):
     # boxes run their x boundary columns in a launch of their own (one node per thread) and
     # the pair kernels over the interior x range: the same sums as the pair kernels with the
@@ -612,7 +613,7 @@ def test_box_x_band_equals_pair_kernels_alone(case):
     else:
         c = dict(order=6, testcase="hall_travelling_wave", nodes=(22, 13, 14), lo=0.0, hi=TWO_PI_, hall=True,
                  integrator="CarpenterKennedy2N54", dt=0.002, real="float" if case.endswith("f32") else "double")
-        if "hod" in case:
+        if "hod" in case:   # (FP32: the x band of the curl kernel too)
             c.update(dissipation="HIGH_ORDER")
     out = []
     for band in (0, 2):   # never / wherever the rows allow
