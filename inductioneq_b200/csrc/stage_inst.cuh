@@ -127,12 +127,9 @@ static void launch_stage_hall_k(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per,
 
 // the same with two x-adjacent nodes per thread (k_stage_col_x2)
 template <bool P, bool H>
-static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, bool foad, dim3 g,
-                             dim3 b, bool pdl, cudaStream_t s) {
-  if (foad) {
-    if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 1, false, true>, g, b, s, pdl, a);
-    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, false, 0, false, true>, g, b, s, pdl, a);
-  } else if (hod && hodp) {
+static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int conv, bool hodp, dim3 g, dim3 b,
+                             bool pdl, cudaStream_t s) {
+  if (hod && hodp) {
     if (conv) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 1, true>, g, b, s, pdl, a);
     else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, P, H, true, 0, true>, g, b, s, pdl, a);
   } else if (hod) {
@@ -200,17 +197,18 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
     }
     return;
   }
-  // the general pair kernel: periodic Hall runs (with convection or first-order / adaptive
-  // dissipation; measured 25-35 % faster there than one node per thread, whose Hall +
-  // convection build spills at 64 registers).  On boxes and without the Hall term the
+  // the general pair kernel: periodic Hall runs with convection and other flux forms
+  // (measured 25-35 % faster there than one node per thread, whose Hall + convection build
+  // spills at 64 registers; first-order / adaptive dissipation keeps one node per thread:
+  // 64^3 whistler 1.68e10 against 1.53e10 DOF/s).  On boxes and without the Hall term the
   // one-node kernels measured faster (the x boundary rows run per node, and the
   // convection sums of two nodes exceed the registers).
-  if (sh.pairs && per && hall && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
+  if (sh.pairs && per && hall && !foad && a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) &&
       pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
       pair_ok(a.out3)) {
     const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
-    launch_col_x2_ph<true, true>(a, hod, conv, hodp, foad, col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), col_block(ps),
-                                 sh.pdl, s);
+    launch_col_x2_ph<true, true>(a, hod, conv, hodp, col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), col_block(ps), sh.pdl,
+                                 s);
     return;
   }
   // convection without the Hall term, with the reference's default flux forms (product
