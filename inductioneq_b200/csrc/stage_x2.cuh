@@ -1,21 +1,30 @@
-// stage_x2.cuh -- the Hall column kernels with two x-adjacent nodes per thread.
+// stage_x2.cuh -- the column kernels with several x-adjacent nodes per thread.
 //
-// The two kernels of a Hall stage (the curl kernel J = curl(B)/rho, E = J x B and the
-// dissipation sum H; the stage kernel gathering the flux rows on E) are bound by load
-// issue and load latency, not by DRAM bandwidth, at the sizes of this path: the FP32
-// build, with half the bytes, is only a few per cent faster.  Here each thread owns the
-// nodes (ix, ix + 1), ix even.  Every y and z stencil point of both nodes comes from one
-// pair load (16 bytes in FP64), and the x stencils of both nodes from 2*QL+1 pair loads
-// covering ix-2QL .. ix+2QL+1 (QL = ceil(RI/2)), instead of two scalar loads per point and
-// node: about half the load instructions and address arithmetic per node.
+// The kernels of a stage (the curl kernel J = curl(B)/rho, E = J x B and the dissipation
+// sum H; the stage kernel gathering the flux rows) are bound by load issue and load latency,
+// not by DRAM bandwidth, at the sizes of this path: the FP32 build, with half the bytes, was
+// only a few per cent faster with one node per thread.  Here each thread owns K nodes
+// (ix .. ix + K - 1, ix a multiple of K; K = 2 in FP64 and FP32, K = 4 in FP32 on large
+// grids).  Every y and z stencil point of the K nodes comes from one vector load (16 bytes),
+// and their x stencils from 2*QL+1 vector loads covering ix-K*QL .. ix+K*QL+K-1
+// (QL = ceil(RI/K)), instead of one scalar load per point and node: about half the load
+// instructions and address arithmetic per node with pairs.
+//
+//   k_curl_e_x2     curl, E and (HODS) H                              periodic grids; FP32 boxes
+//   k_stage_hall_x2 Hall stage without convection, H precomputed    every grid
+//   k_stage_col_x2  general stage (convection; flux mask fixed at    periodic Hall; Hall +
+//                   compile time for the default forms)               convection, rotation: every grid
+//   k_stage_xband / k_curl_xband   the x boundary columns of a box, one node per thread,
+//                   beside the pair kernels launched over the interior x range (XBAND)
 //
 // Each node's sums are formed term by term in the order of the one-node kernels
-// (k_curl_e, k_curl_e_hod, k_stage_col), so the results are the same.
+// (k_curl_e, k_curl_e_hod, k_stage_col); the results agree with them up to the compiler's
+// choice of fused multiply-adds.
 //
-// A launcher uses these kernels only when every pair is aligned and stays in one row:
-// nx even, each field's component stride even and its base aligned to two elements.
-// x-boundary rows of a non-periodic box (and pairs whose x window would leave the row)
-// take the one-node code per node.
+// A launcher uses these kernels only where every vector load is aligned and stays in one row
+// (nx a multiple of K, each field's component stride a multiple of K, bases aligned to K
+// elements) and where they measured faster (stage_inst.cuh).  Without XBAND, x-boundary rows
+// of a box (and groups whose x window would leave the row) take the one-node code per node.
 #pragma once
 #include "stage_col.cuh"
 
