@@ -821,6 +821,7 @@ void ieq_destroy(ieq_ctx *c) {
   if (c->adj_time) cudaFree(c->adj_time);
   void *own[] = {c->d_tables, c->d_rows_r, c->d_rows_d, c->d_lap_r, c->d_lap_d, c->d_wnorm, c->d_partials,
                  c->d_partials2, c->d_total, c->d_counter, c->d_flag, c->d_cg, c->d_cg_vec, c->d_cg_hist,
+                 c->d_lap_s,
                  c->d_pingpong, c->d_soa};
   for (void *p : own)
     if (p) cudaFree(p);

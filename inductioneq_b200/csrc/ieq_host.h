@@ -101,6 +101,7 @@ struct ieq_ctx {
   void *d_cg = nullptr;            // CgState
   double *d_cg_vec = nullptr;      // FP64 CG vectors: div, phi, r, u, lap (5 x n_pad)
   double *d_cg_hist = nullptr;
+  double *d_lap_s = nullptr;       // the CG Laplacian's rows divided by DX^2, DY^2, DZ^2
   int cg_hist_len = 0;
   void *d_pingpong = nullptr;      // (unused)
   void *d_soa = nullptr;           // structure-of-arrays state of the fused time stepping
