@@ -753,14 +753,6 @@ ieq_status ieq_create(ieq_ctx **out, const char *settings, const char *const *pa
   }
   c->op_id = (c->s.order / 2 - 1) + (c->s.extended ? 3 : 0);
   for (int a = 0; a < 3; ++a) {
-    // a periodic stencil wraps once: its half width (order / 2) must not exceed the nodes
-    // per direction minus one
-    if (c->s.periodic && c->s.nodes[a] < c->op.order / 2 + 1) {
-      g_create_error = "periodic NODES per direction must be at least order/2 + 1 = " +
-                       std::to_string(c->op.order / 2 + 1);
-      delete c;
-      return IEQ_ERR_SHAPE;
-    }
     if (!c->s.periodic && c->s.nodes[a] < 2 * c->op.nb) {
       g_create_error = "NODES per direction must be at least 2*NUM_BOUNDS = " + std::to_string(2 * c->op.nb);
       delete c;

@@ -14,8 +14,8 @@ def pytest_configure(config):
 
 
 def pytest_collection_modifyitems(config, items):
-    # GPU tests are skipped cleanly when no device is visible; the round-end GPU run
-    # selects them with -m gpu on a machine that has one.
+    # GPU tests are skipped cleanly when no device is visible; a run on a machine with a
+    # GPU selects them with -m gpu.
     try:
         import torch
         has_gpu = torch.cuda.is_available()

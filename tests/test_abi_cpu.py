@@ -52,8 +52,8 @@ BASE = " -DNODES_X=16 -DNODES_Y=16 -DNODES_Z=16 -DXMIN=0 -DXMAX=1 -DYMIN=0 -DYMA
      1, "narrow-stencil"),
     (BASE + " -DIEQ_INTEGRATOR=RK4", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "integrator"),
     (BASE.replace("=16", "=10"), ["../include/6thOrder.h", "../include/rotation_3D.h"], 2, "2*NUM_BOUNDS"),
-    (BASE.replace("=16", "=3") + " -DUSE_PERIODIC=1", ["../include/6thOrder.h", "../include/rotation_3D.h"], 2,
-     "order/2 + 1"),
+    (BASE.replace("=16", "=10") + " -DUSE_PERIODIC=1", ["../include/6thOrder.h", "../include/rotation_3D.h"], 2,
+     "STENCIL_WIDTH"),
     (BASE + " -DIEQ_COL_BLOCK=32x4x2", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "X * Y * Z = 128"),
     (BASE + " -DIEQ_CURL_BLOCK=32x4", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "XxYxZ"),
     (BASE + " -DIEQ_COL_PAIRS=3", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_COL_PAIRS"),
