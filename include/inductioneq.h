@@ -53,7 +53,14 @@ typedef struct ieq_ctx ieq_ctx;
  *   -DUSE_UIBJ_PRODUCT=1 ... -cl-mad-enable"); OpenCL compiler options are accepted and
  *   ignored.  Keys this library adds (all optional): -DIEQ_INTEGRATOR=<name of one of the
  *   six integrators> (host-side I_TI('time_integrator')), -DIEQ_VARIABLE_U=1
- *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>.
+ *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>;
+ *   and, choosing kernels of the fused time stepping without changing its results beyond
+ *   the compiler's FMA contraction: -DIEQ_STAGE_KERNEL=AUTO|COLUMN|NODE|BRICK|LIST,
+ *   -DIEQ_COL_BLOCK=XxYxZ / -DIEQ_CURL_BLOCK=XxYxZ (128-thread block shapes of the column
+ *   stage and curl kernels), -DIEQ_COL_PAIRS=0|1|4 (nodes per thread: one; the measured
+ *   default; FP32 quads on every grid), -DIEQ_XBAND=0|1|2 (a box's x boundary columns in a
+ *   launch of their own: never, where measured faster, wherever possible), -DIEQ_PDL=0|1
+ *   (programmatic dependent launch of the column kernels).
  * kernel_paths: the kernel_path_list (compute_numerical_solution_setup.m:57-122).  Only
  *   the base names matter: the operator header ({2,4,6}thOrder[Extended].h) selects the SBP
  *   operator, "<testcase>.h" the testcase, artificial_dissipation.cl enables dissipation.
