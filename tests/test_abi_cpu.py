@@ -82,3 +82,21 @@ def test_maps_kernel_path_list_mirrors_setup():
     assert p[0] == "../include/6thOrderExtended.h"
     assert "../kernel/artificial_dissipation.cl" in p
     assert p[-1] == "../kernel/kernel_time_integrator.cl"
+
+
+def test_kernel_selection_settings_are_emitted_and_accepted():
+    # the I_Tech keys of the kernel choices become settings keys the library parses (on a
+    # machine without a GPU ieq_create then stops at the device, not at the settings)
+    m = Maps()
+    m.I_Mesh.update({"NODES_X": 16, "NODES_Y": 16, "NODES_Z": 16, "XMIN": -1.0, "XMAX": 1.0, "YMIN": -1.0,
+                     "YMAX": 1.0, "ZMIN": -1.0, "ZMAX": 1.0})
+    m.I_TI["DT"] = 0.01
+    m.I_RunOps["testcase"] = "rotation_3D"
+    m.I_Tech.update({"stage_kernel": "COLUMN", "col_block": (16, 4, 2), "curl_block": (8, 8, 2), "col_pairs": 4,
+                     "xband": 2, "pdl": 0})
+    s = m.settings()
+    for key in (" -DIEQ_STAGE_KERNEL=COLUMN", " -DIEQ_COL_BLOCK=16x4x2", " -DIEQ_CURL_BLOCK=8x8x2",
+                " -DIEQ_COL_PAIRS=4", " -DIEQ_XBAND=2", " -DIEQ_PDL=0"):
+        assert key in s, key
+    st, err = _create(s, m.kernel_path_list())
+    assert st not in (1, 2), (st, err)    # neither a settings nor a shape error
