@@ -115,22 +115,33 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------ CPU arms
-def cpu_reference_run(steps: int, warmup: int, budget_s: float | None = None):
-    """The reference's own kernels (oracle/_ref, OpenMP over all host cores) on the same
-    workload, one RK step per timed step; returns (DOF-updates/s per stage, cores, kind, sample)."""
+# RK steps of the bench solve in one timed step of the reference arm (a bounded sample of the
+# 260-step solve, so that --steps 20 --warmup 5 ends within seconds on the host cores)
+REF_RK_PER_STEP = 10
+
+
+def cpu_reference_run(steps: int, warmup: int, rk_per_step: int = 1, budget_s: float | None = None,
+                      threads: int | None = None):
+    """The reference's own kernels (oracle/_ref, the -O3 -ffp-contract=fast timing build, OpenMP
+    over the host cores) on the same workload.  One timed step = `rk_per_step` CarpenterKennedy2N54
+    RK steps, timed whole (no extrapolation); with `budget_s` the loop stops after the first step
+    that ends past the budget.  Returns a dict: value (DOF-updates/s per stage), steps run,
+    ms_per_step, cores, kind, build, cpu, sample."""
     import numpy as np
 
     from oracle import refimpl
     from oracle.sequencing import rk_step
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     v = refimpl.Variant(order=6, testcase="hall_circular_wave", periodic=True, hall=True, dissipation="HIGH_ORDER")
     n = N_GRID
     nodes = (n, n, n)
+    build = None
     try:
         mesh = refimpl.Mesh(nodes, (0.0,) * 3, (2 * math.pi,) * 3, periodic=True)
         mesh.dt = DT
-        r = refimpl.RefRunner(v, mesh, nthreads=cores)
+        r = refimpl.RefRunner(v, mesh, nthreads=cores, fast=True)
         kind = "reference"
+        build = f"g++ -O3 -march={refimpl.host_level()} -ffp-contract=fast -fopenmp"
     except Exception:
         r = None
         kind = "port"
@@ -141,23 +152,27 @@ def cpu_reference_run(steps: int, warmup: int, budget_s: float | None = None):
                            dissipation="HIGH_ORDER", testcase="hall_circular_wave", dt=DT)
         r = NumpyOracle(cfg)
         cores = 1
+        build = "numpy restatement"
     b, b2, cb, u = r.vec(), r.vec(), r.vec(), r.vec()
     rho = r.scalar(fill=1.0)
     t = np.zeros(2)
     r.run("init_b", nodes, b)
-    for _ in range(warmup):
+    for _ in range(warmup * rk_per_step):
         r.run_list(seq, nodes, b, b2, cb, u, rho, t)
     t0 = time.perf_counter()
     done = 0
     while done < steps:
-        r.run_list(seq, nodes, b, b2, cb, u, rho, t)
+        for _ in range(rk_per_step):
+            r.run_list(seq, nodes, b, b2, cb, u, rho, t)
         done += 1
-        if budget_s is not None and time.perf_counter() - t0 > budget_s and done >= 3:
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    value = 3 * n ** 3 * STAGES * done / el
-    sample = f"{done} CK2N54 RK steps ({done * STAGES} stages) of the 64^3 workload"
-    return value, cores, kind, sample, el / done * NUM_STEPS_FULL
+    rk = done * rk_per_step
+    return {"value": 3 * n ** 3 * STAGES * rk / el, "steps": done, "ms_per_step": el / done * 1e3, "cores": cores,
+            "kind": kind, "build": build, "cpu": refimpl.cpu_model(), "nproc": os.cpu_count(),
+            "sample": f"{rk} CK2N54 RK steps ({rk * STAGES} stages) of the 64^3 workload, "
+                      f"{rk_per_step} RK step(s) per timed step"}
 
 
 # ------------------------------------------------------------------------------ other forms
@@ -333,13 +348,17 @@ def sharded_batch(rk, dev, steps=200, reps=3):
 
 def form_precision(dev, n=128, steps=20):
     """Confined-domain Hall case on 128^3: FP32 state with FP64 CG cleaning to ||r||_2 < 1e-10,
-    then CK2N54 steps; compared with the FP64 run."""
+    then CK2N54 steps; compared with the FP64 run.  Reported per precision: the weighted
+    ||div B|| (sqrt(norm2_S(calc_div B))) before and right after the projection and after the
+    steps; and the mass-weighted L2 difference of the FP32 field from the FP64 field, after
+    the projection and after the steps."""
     import numpy as np
     import torch
 
     from inductioneq_b200.induction_eq import Maps
     out = {}
     fields = {}
+    ctxs = {}
     for real in ("double", "float"):
         m = Maps()
         m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": 0.0, "XMAX": 1.0, "YMIN": 0.0,
@@ -351,22 +370,29 @@ def form_precision(dev, n=128, steps=20):
         m.I_Tech["REAL"] = real
         m.I_RunOps.update({"order": 4, "testcase": "confined_domain"})
         ctx = m.context(device=dev)
+        ctxs[real] = ctx
         stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
         b = ctx.vec()
         ctx.kernel("init_b", b)
         bh = ctx.get_vec(b).astype(np.float64)
         bh[: ctx.n, :3] += 1e-3 * np.random.default_rng(12345).random((ctx.n, 3))
         b.upload(bh.astype(ctx.real))
+        div_before = ctx.results(b, 0.0, ctx.vec(), ctx.scalar())["divergence_norm"]
         t0 = time.perf_counter()
         cg = ctx.clean_div(b, 20000, 1e-10, check=False)
         cg_s = time.perf_counter() - t0
+        div_after = ctx.results(b, 0.0, ctx.vec(), ctx.scalar())["divergence_norm"]
+        fields[(real, "projected")] = ctx.get_vec(b).astype(np.float64)
         b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec()
         ctx.kernel("init_u", u)
         rho, tt = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+        b_proj = ctx.get_vec(b)
         ctx.time_steps(b, b2, None, cb, u, rho, tt, 2)   # capture + warm
+        b.upload(b_proj)
+        tt.upload(np.zeros(2))
         el = events_time(stream, lambda: ctx.time_steps(b, b2, None, cb, u, rho, tt, steps))
         res = ctx.results(b, 0.0, ctx.vec(), ctx.scalar())
-        fields[real] = ctx.get_vec(b).astype(np.float64)
+        fields[(real, "stepped")] = ctx.get_vec(b).astype(np.float64)
         # the CG loop charged with its compulsory traffic: 80 B per interior node and iteration
         # (a fused two-pass CG: read u, r, write u, lap; read phi, u, r, lap, write phi, r),
         # over the wall clock of the whole cleaning (div B, CG, projection, host polls)
@@ -376,12 +402,119 @@ def form_precision(dev, n=128, steps=20):
                      "cg_residual_norm2": cg["residual_norm2"], "cg_converged": cg["converged"],
                      "cg_wall_s": cg_s, "cg_ms_per_iteration": cg_s / max(cg["iterations"], 1) * 1e3,
                      "cg_achieved_gbs_80B_per_node_iteration": cg_gbs,
-                     "divergence_norm_initial": cg["divergence_norm_initial"],
-                     "divergence_norm_after_steps": res["divergence_norm"]}
-        ctx.close()
-    diff = float(np.abs(fields["float"] - fields["double"]).max() / np.abs(fields["double"]).max())
+                     "cg_residual_initial": cg["divergence_norm_initial"],
+                     "weighted_div_norm_before_projection": div_before,
+                     "weighted_div_norm_after_projection": div_after,
+                     "weighted_div_norm_after_steps": res["divergence_norm"]}
+    # mass-weighted L2 difference of the FP32 field from the FP64 field (norm2_diff of the
+    # FP64 context), relative to the FP64 field's norm
+    c64 = ctxs["double"]
+    l2 = {}
+    for when in ("projected", "stepped"):
+        a, b = c64.vec(fields[("double", when)]), c64.vec(fields[("float", when)])
+        d = c64.norm2_diff(b, a)
+        nrm = c64.norm2(a)
+        l2[when] = {"abs": d ** 0.5, "rel": (d / nrm) ** 0.5}
+    diff = float(np.abs(fields[("float", "stepped")] - fields[("double", "stepped")]).max()
+                 / np.abs(fields[("double", "stepped")]).max())
+    for c in ctxs.values():
+        c.close()
     return {"grid": [n] * 3, "steps": steps, "fp64": out["double"], "fp32_state_fp64_cg": out["float"],
-            "max_rel_diff_fp32_vs_fp64": diff}
+            "l2_diff_fp32_vs_fp64_after_projection": l2["projected"],
+            "l2_diff_fp32_vs_fp64_after_steps": l2["stepped"],
+            "max_rel_diff_fp32_vs_fp64": diff,
+            "note": "weighted div norm = sqrt(norm2_S(calc_div B)) (kernel_operator.cl); L2 diff = "
+                    "sqrt(norm2_diff) relative to sqrt(norm2) of the FP64 field"}
+
+
+def form_rotation40(dev, reps=5):
+    """Linear rotation on 40^3 (the reference's CPU-runnable configuration): [-1, 1]^3, 4th-order
+    SBP, u = (-y, x, 0), divergence-free Gaussian bump, SAT inflow, SSPRK33 at CFL 0.5 to t = 1
+    (dt = 1/56, 56 steps), FP64: DOF-updates/s per stage and the L2 error against the exact
+    rotated field."""
+    import numpy as np
+    import torch
+
+    from inductioneq_b200.induction_eq import Maps
+    n, steps = 40, 56
+    m = Maps()
+    m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": -1.0, "XMAX": 1.0, "YMIN": -1.0,
+                     "YMAX": 1.0, "ZMIN": -1.0, "ZMAX": 1.0})
+    m.I_TI.update({"DT": 1.0 / steps, "time_integrator": "SSPRK33"})
+    m.I_RunOps.update({"order": 4, "testcase": "rotation_gaussian"})
+    ctx = m.context(device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    b, b2, b3, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho, tt = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+    ctx.kernel("init_b", b)
+    ctx.kernel("init_u", u)
+    b0 = ctx.get_vec(b)
+    ctx.time_steps(b, b2, b3, cb, u, rho, tt, steps)   # capture + warm
+    flush = ctx.alloc(256 << 20)
+    tsum = 0.0
+    for k in range(reps):
+        b.upload(b0)
+        tt.upload(np.zeros(2))
+        ctx.memset(flush, k)
+        tsum += events_time(stream, lambda: ctx.time_steps(b, b2, b3, cb, u, rho, tt, steps))
+    res = ctx.results(b, 1.0, ctx.vec(), ctx.scalar())
+    ctx.close()
+    t = tsum / reps
+    return {"grid": [n] * 3, "steps": steps, "dt": 1.0 / steps, "t_final": 1.0, "value": 3 * n ** 3 * 3 * steps / t,
+            "unit": "DOF/s", "ms_per_solve": t * 1e3, "l2_err_vs_exact": {"abs": res["abs_err"], "rel": res["rel_err"]},
+            "note": "the 0.1-wide bump is about 2 dx on this grid: the error is the discretisation error of the "
+                    "configuration, the same as the reference's (parity is tested separately)"}
+
+
+def form_hbm256(dev, n=256, rk_steps=10):
+    """The bench workload's kernels on 256^3 (16.8 M nodes: every field is larger than L2, so
+    the stage runs from HBM): 6th-order SBP + high-order dissipation, Hall, u = 0, periodic,
+    CK2N54, FP64.  The whole stage (every kernel of it) is graded at the stage's compulsory
+    128 B/node, and each kernel at its own traffic."""
+    import numpy as np
+    import torch
+
+    dx = 2 * math.pi / n
+    m = maps(n)
+    m.I_TI.update({"DT": 0.2 * dx * dx})
+    ctx = m.context(device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    b, b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho, tt = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+    ctx.kernel("init_b", b)
+    ctx.time_steps(b, b2, None, cb, u, rho, tt, 2)   # capture + warm
+    el = min(events_time(stream, lambda: ctx.time_steps(b, b2, None, cb, u, rho, tt, rk_steps)) for _ in range(3))
+    prof = ctx.profile_step(b, b2, None, cb, u, rho, tt, repeats=5)
+    ctx.close()
+    peak = _peak_hbm()
+    nn = n ** 3
+    kernels = {}
+    for nm, ms in prof:
+        kernels.setdefault(nm, []).append(ms)
+    per_stage = sum(sum(v) for v in kernels.values()) / STAGES * 1e-3
+    out = {"grid": [n] * 3, "rk_steps": rk_steps, "value": 3 * nn * STAGES * rk_steps / el, "unit": "DOF/s",
+           "ms_per_rk_step": el / rk_steps * 1e3, "stage_ms_sum_of_kernels": per_stage * 1e3,
+           "whole_stage": {"bytes_per_node": STAGE_BYTES_PER_NODE,
+                           "achieved_gbs": STAGE_BYTES_PER_NODE * nn / per_stage / 1e9,
+                           "frac": STAGE_BYTES_PER_NODE * nn / per_stage / 1e9 / peak,
+                           "frac_wall": STAGE_BYTES_PER_NODE * nn * STAGES * rk_steps / el / 1e9 / peak},
+           "peak_gbs": peak, "kernels": {}}
+    own = {"curl_rho": CURL_BYTES_PER_NODE, "stage_2n_fused": 144}
+    for nm, v in kernels.items():
+        ms = statistics.mean(v)
+        rec = {"launches_per_step": len(v), "avg_ms": ms}
+        if nm in own:
+            rec.update({"bytes_per_node": own[nm], "frac": own[nm] * nn / (ms * 1e-3) / 1e9 / peak})
+        out["kernels"][nm] = rec
+    return out
+
+
+def _peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f).get("hbm_gbs") or 6650.0
+    except OSError:
+        return 6650.0
 
 
 def form_adjoint(dev, n=64, t_final=0.2, every=10, n_dirs=20):
@@ -495,6 +628,9 @@ def main() -> None:
                     help="one node per thread in the Hall column kernels (IEQ_COL_PAIRS=0)")
     ap.add_argument("--sharded-batch", action="store_true",
                     help="only the batched form, its 32 solves split between the ranks")
+    ap.add_argument("--form", default=None,
+                    help="run only this form (fp32, rotation_c1, hbm_256, batched, precision_c3, adjoint_c5) "
+                         "on one GPU and print its JSON")
     a = ap.parse_args()
     from inductioneq_b200 import ranks as R
     rk = R.Ranks.from_env()
@@ -503,16 +639,20 @@ def main() -> None:
     if a.impl == "reference":
         if rank != 0:
             return
-        # each timed step is a bounded sample (5 RK steps) of one solve; ms_per_step is
-        # scaled to the full 260-step solve
-        value, cores, kind, sample, s_per_step = cpu_reference_run(5 * a.steps, a.warmup)
+        # each timed step is a bounded sample of the solve: REF_RK_PER_STEP whole RK steps,
+        # timed as they run (ms_per_step is the measured time of one such step)
+        ref = cpu_reference_run(a.steps, a.warmup, rk_per_step=REF_RK_PER_STEP)
+        value = ref["value"]
         print(json.dumps({
-            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": ref["steps"],
+            "warmup": a.warmup, "ms_per_step": ref["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic whistler wave)",
-            "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "stages_per_step": STAGES},
+            "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "stages_per_rk_step": STAGES,
+                       "step": f"a sample of {REF_RK_PER_STEP} CK2N54 RK steps of the 260-step solve"},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": cores, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": ref["cores"], "kind": ref["kind"],
+                             "sample": ref["sample"], "build": ref["build"], "cpu": ref["cpu"],
+                             "nproc": ref["nproc"]},
             "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
         return
@@ -523,6 +663,12 @@ def main() -> None:
     R.init(rk, "nccl", timeout_s=120.0)
     dev = local_rank
     torch.cuda.set_device(dev)
+    if a.form:
+        forms = {"rotation_c1": form_rotation40, "hbm_256": form_hbm256, "batched": form_batched,
+                 "precision_c3": form_precision, "adjoint_c5": form_adjoint}
+        print(json.dumps({a.form: forms[a.form](dev)}))
+        R.finish(rk)
+        return
     if a.sharded_batch:
         line = sharded_batch(rk, dev)
         if rank == 0:
@@ -709,14 +855,18 @@ def main() -> None:
             out["forms"] = {"fp32": form_fp32(dev, b_ref)}
         except Exception as e:   # a form that fails is reported, not fatal to the line
             out["forms"] = {"fp32": {"error": repr(e)}}
-        for name, fn in (("batched", form_batched), ("precision_c3", form_precision), ("adjoint_c5", form_adjoint)):
+        for name, fn in (("rotation_c1", form_rotation40), ("hbm_256", form_hbm256), ("batched", form_batched),
+                         ("precision_c3", form_precision), ("adjoint_c5", form_adjoint)):
             try:
                 out["forms"][name] = fn(dev)
             except Exception as e:
                 out["forms"][name] = {"error": repr(e)}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cv, cores, kind, sample, _ = cpu_reference_run(10 ** 6, 1, budget_s=15.0)
-        out["cpu_baseline"] = {"value": cv, "unit": "DOF/s", "cores": cores, "kind": kind, "sample": sample}
+        ref = cpu_reference_run(10 ** 6, 1, budget_s=15.0)
+        one = cpu_reference_run(10 ** 6, 1, budget_s=4.0, threads=1)
+        out["cpu_baseline"] = {"value": ref["value"], "unit": "DOF/s", "cores": ref["cores"], "kind": ref["kind"],
+                               "sample": ref["sample"], "build": ref["build"], "cpu": ref["cpu"],
+                               "nproc": ref["nproc"], "one_core": {"value": one["value"], "sample": one["sample"]}}
     if rank == 0:
         print(json.dumps(out))
     ctx.close()

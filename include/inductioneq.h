@@ -157,6 +157,15 @@ ieq_status ieq_compute_results(ieq_ctx *ctx, const void *b, double t, void *work
 /* IEQ_ERR_NAN if any x/y/z component of the vector field is not finite, else IEQ_OK. */
 ieq_status ieq_check_finite(ieq_ctx *ctx, const void *vec_field);
 
+/* Test hook of the TMA brick kernels' bounded mbarrier waits (failure-path tests): with
+ * first_wait_gives_up = 1 every brick's first wait for its halo copies gives up at once, so
+ * the brick records a time-out, waits for its copies with the production limit before it
+ * leaves (no copy is left writing into shared memory) and the next ieq_time_steps returns
+ * IEQ_ERR_TIMEOUT; 0 restores the production waits.  A brick that leaves with copies still
+ * outstanding after that second wait is reported as a different IEQ_ERR_TIMEOUT message:
+ * the context's results are then undefined and it should be destroyed. */
+ieq_status ieq_test_brick_wait(ieq_ctx *ctx, int first_wait_gives_up);
+
 /* Profiling (the per-kernel counterpart of the kernel time MatCL returns): every launch of
  * one ieq_time_steps step is captured alone, `repeats` times back to back, into a CUDA graph
  * and timed with events around the graph; records[k] gets the label and average device
@@ -202,6 +211,12 @@ ieq_status ieq_batch_run(ieq_batch *batch, int num_steps, int mode);
 ieq_status ieq_batch_unbind(ieq_batch *batch);
 long long ieq_batch_total_tiles(const ieq_batch *batch);
 int ieq_batch_grid(const ieq_batch *batch);
+/* Test hook of the persistent mode's bounded grid barrier (failure-path tests): every later
+ * ieq_batch_run waits for `extra_arrivals` (0 or 1) blocks beyond the grid -- 1 is a block
+ * that never arrives, so each wait runs out after `spin_limit` 64-ns sleeps (<= 0: the
+ * production limit, about 1.3 s) and the run returns IEQ_ERR_TIMEOUT.  (0, 0) restores the
+ * production barrier; every run starts from a reset barrier state. */
+ieq_status ieq_batch_test_barrier(ieq_batch *batch, int extra_arrivals, long long spin_limit);
 
 /* ---------------------------------------------------------------- discrete adjoint */
 
@@ -239,8 +254,10 @@ ieq_status ieq_adjoint_steps(ieq_ctx *ctx, const void *b0, void *lambda, const v
  * device image, which every GPU that loads the library holds until the process exits.
  *   - n may be at most IEQ_NOALLOC_DOT_MAX_ELEMENTS; larger n returns IEQ_ERR_SHAPE and
  *     launches nothing.  NULL pointers return IEQ_ERR_ARG.
- *   - The first call on a device looks up the scratch array's device address (once per
- *     device, with that device current); make that first call before any stream capture.
+ *   - Every call looks up the scratch array's device address for the calling thread's
+ *     current device (cudaGetSymbolAddress, which allocates nothing); the first call on a
+ *     device also loads the library's device image there, so make it before any stream
+ *     capture.
  *   - All calls share the one scratch array, which keeps the last call's partials.  Every
  *     partial a call reads was written earlier in that call, so nothing needs clearing, but
  *     calls that overlap on the GPU (other streams, other threads) race: order them.

@@ -70,6 +70,7 @@ class Batch:
         lib.ieq_batch_total_tiles.argtypes = [vp]
         lib.ieq_batch_total_tiles.restype = ctypes.c_longlong
         lib.ieq_batch_grid.argtypes = [vp]
+        lib.ieq_batch_test_barrier.argtypes = [vp, ctypes.c_int, ctypes.c_longlong]
         self.specs = list(specs)
         self.ctxs = [rotation_maps(*s).context(device) for s in self.specs]
         arr = (vp * len(self.ctxs))(*[c.h for c in self.ctxs])
@@ -117,6 +118,10 @@ class Batch:
         (one graph branch per solve); `persistent` picks between the first two."""
         m = self.MODES[mode] if mode is not None else (1 if persistent else 0)
         self._check(self.lib.ieq_batch_run(self.h, int(steps), m))
+
+    def test_barrier(self, extra_arrivals: int, spin_limit: int = 0):
+        """Failure-path test hook of the persistent mode's grid barrier (ieq_batch_test_barrier)."""
+        self._check(self.lib.ieq_batch_test_barrier(self.h, int(extra_arrivals), int(spin_limit)))
 
     def unbind(self):
         self._check(self.lib.ieq_batch_unbind(self.h))

@@ -27,11 +27,15 @@ struct BatchSolveDesc {
   double dt;
 };
 
+// the grid barrier's state, reset before every run: arrival count, generation, error flag,
+// and its wait parameters -- arrivals the barrier expects beyond the grid (0; a test sets 1
+// to make every wait run out) and the spin limit of a wait
 struct BatchSync {
   unsigned count;
   unsigned generation;
   int error;
-  int pad;
+  int extra;
+  long long spin_limit;
 };
 
 // resident blocks of 256 threads per SM the batched kernels are compiled for
@@ -50,7 +54,8 @@ __device__ bool grid_barrier(BatchSync *sync, Last last) {
     volatile unsigned *gen = &sync->generation;
     const unsigned g = *gen;
     __threadfence();
-    if (atomicAdd(&sync->count, 1u) == gridDim.x - 1) {
+    const long long limit = sync->spin_limit;
+    if (atomicAdd(&sync->count, 1u) == gridDim.x - 1 + (unsigned)sync->extra) {
       last();
       sync->count = 0;
       __threadfence();
@@ -58,7 +63,7 @@ __device__ bool grid_barrier(BatchSync *sync, Last last) {
     } else {
       long long it = 0;
       while (*gen == g) {
-        if (++it > kBarrierSpinLimit) {
+        if (++it > limit) {
           atomicExch(&sync->error, 1);
           break;
         }
@@ -185,6 +190,7 @@ struct ieq_batch {
   std::vector<void *> bound;
   cudaEvent_t fork = nullptr;          // IEQ_BATCH_BRANCHES: fork/join of the solves' streams
   std::vector<cudaEvent_t> join;
+  BatchSync sync_init{0u, 0u, 0, 0, kBarrierSpinLimit};   // copied to d_sync before every run
 };
 
 // from api.cu / api_fused.inc
@@ -395,6 +401,10 @@ ieq_status ieq_batch_run(ieq_batch *b, int num_steps, int mode) {
       b->graph_persistent = mode;
     }
   }
+  // a fresh barrier state for every run: a run after a time-out starts from a zero count
+  // and a clear error flag
+  if (cudaMemcpyAsync(b->d_sync, &b->sync_init, sizeof(BatchSync), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+    return bfail(b, IEQ_ERR_CUDA, "barrier reset");
   if (num_steps > 0 && cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return bfail(b, IEQ_ERR_CUDA, "launch");
   BatchSync hs{};
   if (cudaMemcpyAsync(&hs, b->d_sync, sizeof(hs), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
@@ -417,6 +427,17 @@ ieq_status ieq_batch_unbind(ieq_batch *b) {
 }
 
 int ieq_batch_grid(const ieq_batch *b) { return b ? b->grid : 0; }
+
+// Test hook of the persistent mode's grid barrier: the barrier then waits for `extra_arrivals`
+// blocks beyond the grid (1: a block that never comes, so every wait runs out) with a spin
+// limit of `spin_limit` 64-ns sleeps (<= 0: the default, about 1.3 s).  (0, 0) restores the
+// production barrier.
+ieq_status ieq_batch_test_barrier(ieq_batch *b, int extra_arrivals, long long spin_limit) {
+  if (!b || extra_arrivals < 0 || extra_arrivals > 1) return IEQ_ERR_ARG;
+  b->sync_init.extra = extra_arrivals;
+  b->sync_init.spin_limit = spin_limit > 0 ? spin_limit : kBarrierSpinLimit;
+  return IEQ_OK;
+}
 
 long long ieq_batch_total_tiles(const ieq_batch *b) { return b ? b->ntiles : 0; }
 

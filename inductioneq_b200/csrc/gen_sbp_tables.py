@@ -154,7 +154,13 @@ def emit_inc(data: dict) -> str:
 
 
 def main() -> None:
-    inc_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/include"
+    # the reference's include directory: the first argument, else $IEQ_REFERENCE_DIR/include
+    if len(sys.argv) > 1:
+        inc_dir = sys.argv[1]
+    elif os.environ.get("IEQ_REFERENCE_DIR"):
+        inc_dir = os.path.join(os.environ["IEQ_REFERENCE_DIR"], "include")
+    else:
+        sys.exit("usage: gen_sbp_tables.py <reference include directory> (or set IEQ_REFERENCE_DIR)")
     data = build(inc_dir)
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "sbp_tables.inc"), "w") as f:

@@ -23,10 +23,10 @@ constexpr int kMaxBlocks = IEQ_NOALLOC_DOT_MAX_ELEMENTS / kPerBlock;  // 4096 pa
 // the scratch: one partial per block; every GPU that loads the library holds it until exit
 __device__ __align__(256) double g_noalloc_partials[kMaxBlocks];
 
-// host-side stand-in names are not device addresses: the address is looked up once per
-// device with that device current
-constexpr int kMaxDevices = 64;
-double *g_partials_addr[kMaxDevices] = {nullptr};
+// In host code the array's name is a host-side stand-in, not a device address: the address
+// is looked up with cudaGetSymbolAddress (which allocates nothing) on every call, with the
+// calling thread's current device, so a module reloaded after a device reset is found again.
+// The lock serialises the lookups (the first one on a device loads the library's device image).
 std::mutex g_setup_mutex;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -73,22 +73,24 @@ extern "C" ieq_status ieq_dot_product_noalloc(const double *a, const double *b, 
                                               void *stream) {
   if (!result || (n > 0 && (!a || !b))) return IEQ_ERR_ARG;
   if (n > (uint64_t)IEQ_NOALLOC_DOT_MAX_ELEMENTS) return IEQ_ERR_SHAPE;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return IEQ_ERR_CUDA;
   double *partials = nullptr;
   {
-    // set-up on the first call on this device (no allocation: only the symbol's address)
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
-      void *p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return IEQ_ERR_CUDA;
-      g_partials_addr[dev] = static_cast<double *>(p);
-    }
-    partials = g_partials_addr[dev];
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return IEQ_ERR_CUDA;
+    partials = static_cast<double *>(p);
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int nblocks = (int)((n + kPerBlock - 1) / kPerBlock);
-  if (nblocks > 0) k_dot_partials<<<nblocks, kThreads, 0, s>>>(a, b, (long long)n, partials);
-  k_dot_final<<<1, kThreads, 0, s>>>(partials, nblocks, result);
-  return cudaGetLastError() == cudaSuccess ? IEQ_OK : IEQ_ERR_CUDA;
+  long long nn = (long long)n;
+  int nblocks = (int)((nn + kPerBlock - 1) / kPerBlock);
+  // each launch's own status (not an error left behind by an earlier, unrelated launch)
+  if (nblocks > 0) {
+    void *args[] = {(void *)&a, (void *)&b, (void *)&nn, (void *)&partials};
+    if (cudaLaunchKernel((const void *)k_dot_partials, dim3(nblocks), dim3(kThreads), args, 0, s) != cudaSuccess)
+      return IEQ_ERR_CUDA;
+  }
+  void *fargs[] = {(void *)&partials, (void *)&nblocks, (void *)&result};
+  if (cudaLaunchKernel((const void *)k_dot_final, dim3(1), dim3(kThreads), fargs, 0, s) != cudaSuccess)
+    return IEQ_ERR_CUDA;
+  return IEQ_OK;
 }

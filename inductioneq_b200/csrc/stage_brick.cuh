@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   const int lx = t % kBX, ly = (t / kBX) % kBY, lz0 = t / (kBX * kBY);
   const bool aligned = (smem_u32(smem) & 127u) == 0;
   if (!brick_interior<OP, PER>(x0, y0, z0, nx, ny, nz) || !aligned) {
-    if (!aligned && t == 0) atomicExch(err, 2);   // no copy is issued into a misaligned buffer
+    if (!aligned && t == 0) atomicMax(err, kBrickErrMisaligned);   // no copy is issued into a misaligned buffer
 #pragma unroll
     for (int k = 0; k < kBrickNodesPerThread; ++k) {
       const int ix = x0 + lx, iy = y0 + ly, iz = z0 + lz0 + kBrickZPerPass * k;
@@ -100,14 +100,11 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     ein[k] = epilogue_load(a, (x0 + lx) + (long long)nx * ((y0 + ly) + (long long)ny * iz));
   }
   __syncthreads();
-  if (!mbar_wait_bounded(bar, 0)) {
-    *ok = 0;
-    atomicExch(err, 1);
-  }
+  if (!brick_first_wait(bar, err)) *ok = 0;
   __syncthreads();
   if (!*ok) {
     // leave only after the copies stopped writing into this CTA's shared memory
-    mbar_wait_bounded(bar, 0);
+    brick_drain(bar, err);
     stage_time_post(a);
     return;
   }
@@ -192,7 +189,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       stf(a.jface, idx, J);
   };
   if (!brick_interior<OP, PER>(x0, y0, z0, nx, ny, nz) || !aligned) {
-    if (!aligned && t == 0) atomicExch(err, 2);
+    if (!aligned && t == 0) atomicMax(err, kBrickErrMisaligned);
 #pragma unroll
     for (int k = 0; k < kBrickNodesPerThread; ++k) {
       const int ix = x0 + lx, iy = y0 + ly, iz = z0 + lz0 + kBrickZPerPass * k;
@@ -239,13 +236,10 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     *ok = 1;
   }
   __syncthreads();
-  if (!mbar_wait_bounded(bar, 0)) {
-    *ok = 0;
-    atomicExch(err, 1);
-  }
+  if (!brick_first_wait(bar, err)) *ok = 0;
   __syncthreads();
   if (!*ok) {
-    mbar_wait_bounded(bar, 0);
+    brick_drain(bar, err);
     return;
   }
   if (PER && (x0 == 0 || x0 + kBX == nx)) {

@@ -92,6 +92,29 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
   return false;
 }
 
+// The brick kernels' error word err[0] (the highest code wins): 1 a brick's first wait
+// for its halo copies gave up (the brick skipped its computation; its copies completed
+// before it left), 2 a misaligned shared-memory buffer (the brick ran on the global path),
+// 3 copies still outstanding when a brick left after its second wait (they may have
+// written into the shared memory of a later CTA: the context's results are undefined).
+// err[kBrickHookSlot] is a test hook: non-zero makes every first wait give up at once.
+constexpr int kBrickErrLate = 1, kBrickErrMisaligned = 2, kBrickErrOutstanding = 3;
+constexpr int kBrickHookSlot = 6;
+
+// the first bounded wait of a brick for phase 0; false (recorded in err) if it gave up
+__device__ __forceinline__ bool brick_first_wait(uint64_t *bar, int *err) {
+  const bool give_up = *reinterpret_cast<volatile int *>(err + kBrickHookSlot) != 0;
+  if (!give_up && mbar_wait_bounded(bar, 0)) return true;
+  atomicMax(err, kBrickErrLate);
+  return false;
+}
+
+// after a brick gave up: wait (production limit) until its copies stopped writing into
+// its shared memory before it leaves; record the case where they did not
+__device__ __forceinline__ void brick_drain(uint64_t *bar, int *err) {
+  if (!mbar_wait_bounded(bar, 0)) atomicMax(err, kBrickErrOutstanding);
+}
+
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z,
                                             int c) {
   asm volatile(

@@ -86,6 +86,7 @@ def load() -> ctypes.CDLL:
         getattr(lib, f).argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
     lib.ieq_compute_results.argtypes = [vp, vp, ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_double * 4)]
     lib.ieq_check_finite.argtypes = [vp, vp]
+    lib.ieq_test_brick_wait.argtypes = [vp, ctypes.c_int]
     lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.POINTER(KernelRecord),
                                                 ctypes.POINTER(ctypes.c_int)]
     lib.ieq_operator_jvp.argtypes = [vp] * 6
@@ -309,6 +310,10 @@ class Context:
 
     def check_finite(self, b) -> None:
         self._check(self.lib.ieq_check_finite(self.h, _ptr(b)))
+
+    def test_brick_wait(self, first_wait_gives_up: bool) -> None:
+        """Failure-path test hook of the TMA brick kernels' waits (ieq_test_brick_wait)."""
+        self._check(self.lib.ieq_test_brick_wait(self.h, 1 if first_wait_gives_up else 0))
 
 
 def fp64_fma_rate(device: int = 0, iterations: int = 20000) -> float:

@@ -25,7 +25,10 @@ REF_OUT = os.path.join(HERE, "_ref")
 DRIVER = os.path.join(HERE, "ref", "ref_driver.cpp")
 SHIM_DIR = os.path.join(HERE, "ref")
 OWN_TESTCASES = os.path.join(HERE, "ref", "testcases")
-REFERENCE_DIR = os.environ.get("IEQ_REFERENCE_DIR", "/root/reference")
+# the reference checkout: IEQ_REFERENCE_DIR, else a directory named "reference" beside this
+# repository's root
+REFERENCE_DIR = os.environ.get("IEQ_REFERENCE_DIR",
+                               os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 
 REFERENCE_TESTCASES = ("rotation_2D", "rotation_3D", "hall_periodic", "hall_travelling_wave",
                        "confined_domain", "alfven_periodic_2D")
@@ -71,17 +74,53 @@ class Variant:
         return tag
 
 
-def _lib_path(v: Variant) -> str:
-    return os.path.join(REF_OUT, f"ref_{v.key()}.so")
+# Two builds of every variant:
+#   strict (parity): -O2 -ffp-contract=off, the reference's evaluation order without fused
+#     multiply-adds -- the oracle the tests compare against;
+#   fast (timing): -O3 -ffp-contract=fast with the widest x86-64 level the host supports
+#     (x86-64-v4: AVX-512; x86-64-v3: AVX2 + FMA), the build the CPU baseline and the
+#     reference arm of bench.py time.  -march=native cannot be used: the library is built on
+#     one machine and timed on another, whose CPU model may differ; both levels are built
+#     and the one the running host supports is loaded.
+FAST_LEVELS = ("x86-64-v4", "x86-64-v3")
+
+
+def host_level() -> str:
+    """x86-64-v4 if the running CPU has the AVX-512 subsets that level needs, else v3."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln.split(":", 1)[1].split() for ln in f if ln.startswith("flags")), [])
+    except OSError:
+        flags = []
+    need = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+    return "x86-64-v4" if all(x in flags for x in need) else "x86-64-v3"
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _lib_path(v: Variant, level: str | None = None) -> str:
+    if level is None:
+        return os.path.join(REF_OUT, f"ref_{v.key()}.so")
+    return os.path.join(REF_OUT, f"ref_{v.key()}_fast_{level.replace('-', '')}.so")
 
 
 def reference_available() -> bool:
     return os.path.isfile(os.path.join(REFERENCE_DIR, "kernel", "kernel_time_integrator.cl"))
 
 
-def build(v: Variant, force: bool = False) -> str:
-    """Compile the variant from the reference sources in place; returns the .so path."""
-    out = _lib_path(v)
+def build(v: Variant, force: bool = False, level: str | None = None) -> str:
+    """Compile the variant from the reference sources in place; returns the .so path.
+    level None: the strict parity build; an x86-64 level: the fast timing build."""
+    out = _lib_path(v, level)
     if os.path.isfile(out) and not force:
         return out
     if not reference_available():
@@ -89,7 +128,8 @@ def build(v: Variant, force: bool = False) -> str:
                            f"variant {v.key()} was not built beforehand")
     os.makedirs(REF_OUT, exist_ok=True)
     tmp = out + f".{os.getpid()}.tmp"
-    cmd = ["g++", "-O2", "-std=gnu++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off", "-w",
+    opt = ["-O2", "-ffp-contract=off"] if level is None else ["-O3", f"-march={level}", "-ffp-contract=fast"]
+    cmd = ["g++", *opt, "-std=gnu++17", "-fopenmp", "-fPIC", "-shared", "-w",
            f"-I{SHIM_DIR}", f"-I{REFERENCE_DIR}/include", f"-I{REFERENCE_DIR}/kernel",
            f"-I{OWN_TESTCASES}", *v.defines(), DRIVER, "-o", tmp]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
@@ -100,8 +140,13 @@ def build(v: Variant, force: bool = False) -> str:
 _LIBS: dict[str, ctypes.CDLL] = {}
 
 
-def load(v: Variant) -> ctypes.CDLL:
-    path = build(v)
+def build_fast(v: Variant) -> list[str]:
+    """Both fast timing builds of the variant."""
+    return [build(v, level=lv) for lv in FAST_LEVELS]
+
+
+def load(v: Variant, fast: bool = False) -> ctypes.CDLL:
+    path = build(v, level=host_level() if fast else None)
     lib = _LIBS.get(path)
     if lib is None:
         lib = ctypes.CDLL(path)
@@ -148,10 +193,11 @@ class Mesh:
 class RefRunner:
     """Runs reference kernels by name on numpy arrays, like MatCL's cl_run_kernel."""
 
-    def __init__(self, v: Variant, mesh: Mesh, nthreads: int = 1):
+    def __init__(self, v: Variant, mesh: Mesh, nthreads: int = 1, fast: bool = False):
         self.v = v
         self.mesh = mesh
-        self.lib = load(v)
+        self.fast = fast
+        self.lib = load(v, fast)
         self.nthreads = nthreads
         self.dtype = np.float32 if v.real == "float" else np.float64
         nodes = (ctypes.c_uint * 3)(*mesh.nodes)

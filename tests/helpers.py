@@ -54,3 +54,21 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     """max |a - b| / max(|b|): the per-stage relative error of a field."""
     scale = float(np.abs(b).max())
     return float(np.abs(a - b).max()) / (scale if scale > 0 else 1.0)
+
+
+def ref_runner_for(c: dict, dt=None):
+    """The reference's kernels compiled in place (the strict parity build of oracle/_ref),
+    OpenMP over every host core, for one case description."""
+    import os
+
+    from oracle import refimpl
+    m = mesh_args(c)
+    mesh = refimpl.Mesh(m["nodes"], m["xmin"], m["xmax"], m["periodic"],
+                        dt=c.get("dt", 0.0) if dt is None else dt, bnodes=c.get("bnodes", 1),
+                        tc_omega=c.get("omega", 1.0))
+    return refimpl.RefRunner(refimpl.Variant(**variant_kwargs(c)), mesh, nthreads=os.cpu_count() or 1)
+
+
+def own_scale_err(got: np.ndarray, ref: np.ndarray) -> float:
+    """max |got - ref| / max |ref| over the first len(ref) rows (the device arrays are padded)."""
+    return rel_err(np.asarray(got)[: len(ref)].astype(np.float64), ref.astype(np.float64))

@@ -220,13 +220,8 @@ def test_fused_column_kernel_cases(name):
               host[3], host[4], host[5], host[6])
     ctx.time_steps(*dev, c["steps"])
     for i in (0, 1, 3) if hall else (0, 1):
-        got = ctx.get_vec(dev[i])
-        if i == 1:
-            # b2 holds DT * DB; the dissipation rows cancel the unit mean field B_z = 1, so
-            # its rounding is on the scale of the state, not of the (small) increment
-            e = float(np.abs(got - host[1]).max()) / float(np.abs(host[0]).max())
-        else:
-            e = rel_err(got, host[i])
+        # every field on its own scale, the RK register b2 (= DT x DB for the 2N schemes) included
+        e = rel_err(ctx.get_vec(dev[i]), host[i])
         assert e <= tol(c), (i, e)
     assert rel_err(host[0], bh) > 1e-6
     np.testing.assert_allclose(ctx.get_scalar(dev[6], n=2), host[6], rtol=1e-15 if o.T == np.float64 else 1e-6)
@@ -267,10 +262,8 @@ def test_fused_hall_convection_pairs_match_oracle(name):
     time_loop(o, c["integrator"], True, False, c["steps"], host[0], host[1], host[2] if nf == 3 else None,
               host[3], host[4], host[5], host[6])
     ctx.time_steps(*dev, c["steps"])
-    scale = float(np.abs(host[0]).max())
     for i in (0, 1, 3):
-        got = ctx.get_vec(dev[i])
-        e = float(np.abs(got - host[i]).max()) / (scale if i == 1 else float(np.abs(host[i]).max()))
+        e = rel_err(ctx.get_vec(dev[i]), host[i])
         assert e <= tol(c), (i, e)
     assert rel_err(host[0], bh) > 1e-7
 
@@ -326,7 +319,7 @@ def test_fused_steps_equal_reference_kernel_lists(name):
         ctx.time_steps(*dev, 3)
         out.append([ctx.get_vec(dev[i]) for i in range(nf)] + [ctx.get_scalar(dev[6], n=2)])
     for i in range(nf):
-        assert rel_err(out[0][i], out[1][i]) <= 10 * tol(c), i
+        assert rel_err(out[0][i], out[1][i]) <= tol(c), (i, rel_err(out[0][i], out[1][i]))
     np.testing.assert_allclose(out[0][-1], out[1][-1], rtol=1e-15)
 
 
@@ -515,10 +508,9 @@ def test_fused_hall_hod_steps_equal_kernel_lists_for_every_integrator(integrator
         ctx.time_steps(*dev, 3)
         out.append([ctx.get_vec(dev[i]).astype(np.float64) for i in range(nf)] + [ctx.get_vec(dev[3]), 
                    ctx.get_scalar(dev[6], n=2)])
-    scale = float(np.abs(out[1][0]).max())
     for i in range(nf + 1):
-        # fields compared on the state's scale (b2 of the 2N schemes holds DT x DB)
-        e = float(np.abs(out[0][i] - out[1][i]).max()) / scale
+        # every field on its own scale (b2 of the 2N schemes holds DT x DB)
+        e = rel_err(out[0][i].astype(np.float64), out[1][i].astype(np.float64))
         assert e <= (1e-12 if real == "double" else 2e-6), (i, e)
     np.testing.assert_allclose(out[0][-1], out[1][-1], rtol=1e-15 if real == "double" else 1e-6)
 
@@ -590,10 +582,9 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
         ctx.kernel("init_u", dev[4])
         ctx.time_steps(*dev, 3)
         out.append([ctx.get_vec(dev[0]), ctx.get_vec(dev[1]), ctx.get_vec(dev[3])])
-    scale = float(np.abs(out[0][0]).max())
     tol = 2e-6 if case.endswith("f32") else 1e-13
     for i, (a, b) in enumerate(zip(*out)):
-        e = float(np.abs(a.astype(np.float64) - b).max()) / scale
+        e = rel_err(a.astype(np.float64), b.astype(np.float64))
         assert e <= tol, (i, e)
     assert np.isfinite(out[0][0]).all()
 
@@ -624,10 +615,9 @@ def test_box_x_band_equals_pair_kernels_alone(case):
         ctx.kernel("init_u", dev[4])
         ctx.time_steps(*dev, 3)
         out.append([ctx.get_vec(dev[0]), ctx.get_vec(dev[1]), ctx.get_scalar(dev[6], n=2)])
-    scale = float(np.abs(out[0][0]).max())
     tol = 2e-6 if c.get("real") == "float" else 1e-13
     for i in (0, 1):
-        e = float(np.abs(out[0][i].astype(np.float64) - out[1][i]).max()) / scale
+        e = rel_err(out[0][i].astype(np.float64), out[1][i].astype(np.float64))
         assert e <= tol, (i, e)
     np.testing.assert_array_equal(out[0][2], out[1][2])    # time bookkeeping by the band kernel
     assert np.isfinite(out[1][0]).all()

@@ -55,6 +55,35 @@ def test_noalloc_dot_matches_context_dot_on_two_calls():
         assert abs(got - exact) <= TOL * np.sum(np.abs(ah[:n] * bh[:n])), (call, got, exact)
 
 
+@pytest.mark.parametrize("grid, trim", [((100, 101, 102), 0), ((128, 256, 256), 0), ((128, 256, 256), 1)])
+def test_noalloc_dot_at_large_sizes_matches_context_dot(grid, trim):
+    # n above 256 partial blocks (the final kernel's strided loop over the partials) up to the
+    # stated maximum, and one element below it; the context's dot runs over all its nodes, so
+    # with trim = 1 the last element of b is zero there and absent from the no-alloc call
+    m = Maps()
+    m.I_Mesh.update({"NODES_X": grid[0], "NODES_Y": grid[1], "NODES_Z": grid[2], "XMIN": 0.0, "XMAX": 1.0,
+                     "YMIN": 0.0, "YMAX": 1.0, "ZMIN": 0.0, "ZMAX": 1.0})
+    m.I_RunOps.update({"order": 2, "testcase": "confined_domain"})
+    ctx = m.context()
+    n = ctx.n - trim
+    assert n <= 8388608 and (n > 524288)
+    rng = np.random.default_rng(11)
+    out = ctx.scalar(n=1)
+    for call in range(2):
+        ah = rng.standard_normal(ctx.n_pad)
+        bh = rng.standard_normal(ctx.n_pad) * (1.0 + call)
+        bh[n:] = 0.0
+        a, b = ctx.scalar(ah), ctx.scalar(bh)
+        expected = ctx.dot(a, b)
+        st = _noalloc(ctx.lib, a.ptr, b.ptr, n, out.ptr, ctx.stream)
+        assert st == 0, L.STATUS.get(st, st)
+        ctx.synchronize()
+        got = float(ctx.get_scalar(out, n=1)[0])
+        scale = float(np.sum(np.abs(ah[:n] * bh[:n])))
+        assert abs(got - expected) <= TOL * scale, (call, got, expected)
+    ctx.close()
+
+
 def test_noalloc_dot_refuses_sizes_above_the_maximum():
     ctx = _context(12)
     out = ctx.scalar(n=1)
