@@ -55,7 +55,10 @@ typedef struct ieq_ctx ieq_ctx;
  *   six integrators> (host-side I_TI('time_integrator')), -DIEQ_VARIABLE_U=1
  *   (I_RunOps('variable_u')), -DTC_OMEGA=<rotation rate of the rotation_gaussian case>;
  *   and, choosing kernels of the fused time stepping without changing its results beyond
- *   the compiler's FMA contraction: -DIEQ_STAGE_KERNEL=AUTO|COLUMN|NODE|BRICK|LIST,
+ *   the compiler's FMA contraction: -DIEQ_STAGE_KERNEL=AUTO|COLUMN|NODE|BRICK|LIST|ZMARCH
+ *   (ZMARCH: the one-pass Hall stage that marches through z -- curl, E = J x B, dissipation
+ *   and update in one kernel -- wherever it can run; AUTO takes it on periodic grids of at
+ *   least 2^21 nodes), -DIEQ_ZMARCH_TZ=<z planes per CTA of that kernel; 0 chosen per grid>,
  *   -DIEQ_COL_BLOCK=XxYxZ / -DIEQ_CURL_BLOCK=XxYxZ (128-thread block shapes of the column
  *   stage and curl kernels), -DIEQ_COL_PAIRS=0|1|4 (nodes per thread: one; the measured
  *   default; FP32 quads on every grid), -DIEQ_XBAND=0|1|2 (a box's x boundary columns in a

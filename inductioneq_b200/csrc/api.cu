@@ -10,6 +10,7 @@
 #include "ieq_host.h"
 #include "misc_kernels.cuh"
 #include "stage_brick.cuh"
+#include "stage_z.cuh"
 #include "diag.cuh"
 
 namespace ieq {
@@ -22,6 +23,8 @@ namespace {
 
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs; fixed so that sums are reproducible
 constexpr int kMaxPartials = 65536;  // CG fused-dot partials (one per stencil block)
+// grids from which IEQ_STAGE_KERNEL=AUTO runs the one-pass Hall stage (stage_z.cuh)
+constexpr long long kZmarchAutoNodes = 1LL << 21;
 
 #define IEQ_CUDA(ctx, call)                                                                    \
   do {                                                                                         \
@@ -247,6 +250,19 @@ void launch_stage_col_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, int conv, b
     case 3: launch_stage_col<R, 3>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
     case 4: launch_stage_col<R, 4>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
     case 5: launch_stage_col<R, 5>(a, per, hall, hod, conv, hodp, foad, sh, c->stream); break;
+  }
+}
+
+// the one-pass Hall stage (stage_z.cuh)
+template <typename R>
+void launch_stage_zmarch_any(ieq_ctx *c, const StageArgs<R, SoA<R>> &a, const R *rho, bool hod) {
+  switch (c->op_id) {
+    case 0: launch_stage_zmarch<R, 0>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
+    case 1: launch_stage_zmarch<R, 1>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
+    case 2: launch_stage_zmarch<R, 2>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
+    case 3: launch_stage_zmarch<R, 3>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
+    case 4: launch_stage_zmarch<R, 4>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
+    case 5: launch_stage_zmarch<R, 5>(a, rho, hod, c->s.pdl, c->s.zmarch_tz, c->stream); break;
   }
 }
 
@@ -808,6 +824,9 @@ void ieq_destroy(ieq_ctx *c) {
     if (kv.second.exec1) cudaGraphExecDestroy(kv.second.exec1);
     if (kv.second.exec2) cudaGraphExecDestroy(kv.second.exec2);
   }
+  for (auto &kv : c->clean_graphs)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
+  if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
   for (void *p : c->allocs) cudaFree(p);
   for (void *p : c->adj_bufs) cudaFree(p);
   if (c->adj_time) cudaFree(c->adj_time);

@@ -40,7 +40,9 @@ struct Settings {
   // kernels of the fused time stepping (IEQ_STAGE_KERNEL): 0 AUTO (the column kernels,
   // measured fastest on B200), 1 COLUMN, 2 NODE (the per-node J-based kernels), 3 BRICK
   // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN),
-  // 4 LIST (no fusion: the reference's kernel list of each step on the caller's fields)
+  // 4 LIST (no fusion: the reference's kernel list of each step on the caller's fields),
+  // 5 ZMARCH (the one-pass Hall stage of stage_z.cuh wherever it can run, else COLUMN; AUTO
+  // takes it on grids of at least kZmarchAutoNodes nodes)
   int stage_kernel = 0;
   // thread-block shapes of the column stage kernel (IEQ_COL_BLOCK=XxYxZ) and of the curl
   // kernel (IEQ_CURL_BLOCK); X * Y * Z = 128, all zero for the default 32x4x1
@@ -55,6 +57,8 @@ struct Settings {
   // IEQ_XBAND: boxes run their x boundary columns in a launch of their own -- 0 never, 1
   // (default) where measured faster (the band at most a tenth of the row), 2 wherever possible
   int xband = 1;
+  // IEQ_ZMARCH_TZ: z planes per CTA of the one-pass Hall stage (0: chosen per grid)
+  int zmarch_tz = 0;
 };
 
 // parse helpers (settings.cpp)
@@ -99,7 +103,7 @@ struct ieq_ctx {
   unsigned *d_counter = nullptr;   // last-block tickets
   int *d_flag = nullptr;
   void *d_cg = nullptr;            // CgState
-  double *d_cg_vec = nullptr;      // FP64 CG vectors: div, phi, r, u, lap (5 x n_pad)
+  double *d_cg_vec = nullptr;      // FP64 CG vectors: div, phi, r, u, u', lap (6 x n_pad)
   double *d_cg_hist = nullptr;
   double *d_lap_s = nullptr;       // the CG Laplacian's rows divided by DX^2, DY^2, DZ^2
   int cg_hist_len = 0;
@@ -114,6 +118,10 @@ struct ieq_ctx {
     cudaGraphExec_t exec1 = nullptr, exec2 = nullptr;
   };
   std::map<std::vector<uintptr_t>, GraphEntry> graphs;
+  // cleaning graphs (div B, CG loop as a conditional WHILE node, projection) keyed by the
+  // field and the loop parameters; a second stream on which the loop body is captured
+  std::map<std::vector<uintptr_t>, cudaGraphExec_t> clean_graphs;
+  cudaStream_t aux_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // ieq_profile_step: labels of the step's launches, and a gate that lets only the
   // launch with index gate_target through (-1: all launches, -2: none)

@@ -495,6 +495,150 @@ __global__ void __launch_bounds__(256) k_cg_laplace_fast(const LapArgs<double> a
   }
 }
 
+// ---- the two passes of one CG iteration inside a graph loop (a conditional WHILE node
+// whose condition the last block of pass B sets; no host round trip per iteration).
+//
+// Pass A (clean_div.m:50-56): the search direction u = beta*u + r (calc_axpy) is formed at
+// every stencil point as it is loaded -- u and r are read, the new direction is written at the
+// node into the other buffer of a ping-pong pair (iteration parity) -- and lap = (-Laplace) u,
+// <u, lap> and alpha = rr / <u, lap> (last block) follow in the same pass.  The direction value
+// at a point is __fma_rn(beta, u, r) wherever it is formed, so every node's u is one value.
+// Non-periodic grids: a node whose y and z rows are interior (warp-uniform for x-rows of
+// threads) takes fixed y/z offsets and only its x coefficient from the row table (boundary
+// rows in x no longer send a warp down a second path).
+template <int W>
+__device__ __forceinline__ double cg_dir(const double *uo, const double *r, double beta, long long j) {
+  return __fma_rn(beta, __ldg(uo + j), __ldg(r + j));
+}
+template <int W>
+__device__ __forceinline__ double laplace_dir_at(const LapArgs<double> &a, const LapFastArgs<W> &f, const double *uo,
+                                                 const double *r, double beta, int ix, int iy, int iz, long long idx) {
+  constexpr int C0 = (W - 1) / 2;
+  const int ii[3] = {ix, iy, iz};
+  const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
+  const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
+  const int rows = 2 * a.nb + 1;
+  int row[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) row[ax] = a.periodic ? a.nb : sbp_row(ii[ax], nn[ax], a.nb);
+  double val = 0;
+  if (!a.periodic && row[1] == a.nb && row[2] == a.nb) {
+    const double *lx = f.Ls + (long long)row[0] * W;   // axis 0 rows come first in Ls
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      int jx = ix + c - C0;
+      jx = (jx < 0 || jx >= nn[0]) ? ix : jx;   // clamp-to-self: its coefficient is zero
+      const double t0 = cg_dir<W>(uo, r, beta, idx + (jx - ix)) * lx[c];
+      const double t1 = cg_dir<W>(uo, r, beta, idx + (long long)(c - C0) * st[1]) * f.Li[1][c];
+      const double t2 = cg_dir<W>(uo, r, beta, idx + (long long)(c - C0) * st[2]) * f.Li[2][c];
+      val = ((val + t0) + t1) + t2;
+    }
+    return val;
+  }
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    double t[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const double cf = f.Ls[(ax * rows + row[ax]) * W + c];
+      const long long j = idx + (long long)(nbr_rt<double>(ii[ax], c - C0, nn[ax], a.periodic) - ii[ax]) * st[ax];
+      t[ax] = cg_dir<W>(uo, r, beta, j) * cf;
+    }
+    val = ((val + t[0]) + t[1]) + t[2];
+  }
+  return val;
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_cg_pass_a(const LapArgs<double> a, const LapFastArgs<W> f, const double *r,
+                                                   double *u0, double *u1, CgState *cs, unsigned *counter) {
+  const int it = cs->it;
+  const double *uo = (it & 1) ? u1 : u0;
+  double *un = (it & 1) ? u0 : u1;
+  const double beta = cs->rr / cs->old;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
+  double prod = 0.0;
+  if (ix < a.gx + a.off && iy < a.gy + a.off && iz < a.gz + a.off) {
+    const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
+    const double val = laplace_dir_at<W>(a, f, uo, r, beta, ix, iy, iz, idx);
+    const double uc = cg_dir<W>(uo, r, beta, idx);
+    un[idx] = uc;
+    a.out[idx] = val;
+    prod = uc * val;
+  }
+  if (block_partial_and_ticket(prod, a.partials, counter)) {
+    const int np = gridDim.x * gridDim.y * gridDim.z;
+    const double ul = block_sum_partials(a.partials, np);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+      cs->alpha = cs->rr / ul;
+      *counter = 0u;
+    }
+  }
+}
+
+// Pass B (clean_div.m:57-66): phi += alpha*u (calc_xpay), r -= alpha*lap, rr = <r, r> (last
+// block), then the loop condition of clean_div.m:47, written to the graph loop's condition
+template <typename S>
+__global__ void __launch_bounds__(256) k_cg_pass_b(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,
+                                                   const S *u0, const S *u1, const S *lap, double *partials,
+                                                   CgState *cs, unsigned *counter, double *history,
+                                                   cudaGraphConditionalHandle loop) {
+  const S *u = (cs->it & 1) ? u0 : u1;   // the direction pass A of this iteration wrote
+  const S alpha = (S)cs->alpha;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
+  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
+  double rr = 0.0;
+  if (ix < gx + off && iy < gy + off && iz < gz + off) {
+    const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+    phi[idx] = phi[idx] + alpha * u[idx];
+    const S rn = r[idx] + (-alpha) * lap[idx];
+    r[idx] = rn;
+    rr = (double)rn * (double)rn;
+  }
+  if (block_partial_and_ticket(rr, partials, counter)) {
+    const int np = gridDim.x * gridDim.y * gridDim.z;
+    const double tot = block_sum_partials(partials, np);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+      cs->old = cs->rr;
+      cs->rr = tot;
+      cs->it += 1;
+      if (history) history[cs->it] = tot;
+      cs->done = !(tot > cs->tol && cs->it < cs->max_it);
+      cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
+      *counter = 0u;
+    }
+  }
+}
+
+// the loop state of one cleaning: tolerance and cap (set on the device, so that a captured
+// cleaning needs no host copy)
+static __global__ void k_cg_init(CgState *cs, double tol, int max_it) {
+  if (threadIdx.x == 0) {
+    CgState s{};
+    s.tol = tol;
+    s.max_it = max_it;
+    *cs = s;
+  }
+}
+
+// initial residual r = div B: rr = <r, r> from reduction partials, the loop condition, and
+// the graph loop's condition (no iteration when the field is already clean)
+static __global__ void k_cg_start_loop(const double *partials_rr, int np, CgState *cs, double *history,
+                                       cudaGraphConditionalHandle loop) {
+  const double rr = block_sum_partials(partials_rr, np);
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    cs->rr = rr;
+    cs->old = 1.0;
+    cs->it = 0;
+    if (history) history[0] = rr;
+    cs->done = !(rr > cs->tol && cs->it < cs->max_it);
+    cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
+  }
+}
+
 // phi += alpha*u; r -= alpha*lap; rr = <r, r> (last block), then the loop condition
 template <typename S>
 __global__ void __launch_bounds__(256) k_cg_update(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,

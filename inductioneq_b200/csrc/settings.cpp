@@ -126,7 +126,8 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
       else if (val == "NODE") s.stage_kernel = 2;
       else if (val == "BRICK") s.stage_kernel = 3;
       else if (val == "LIST") s.stage_kernel = 4;
-      else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE, BRICK or LIST"; return false; }
+      else if (val == "ZMARCH") s.stage_kernel = 5;
+      else { err = "IEQ_STAGE_KERNEL must be AUTO, COLUMN, NODE, BRICK, LIST or ZMARCH"; return false; }
     } else if (key == "IEQ_COL_BLOCK" || key == "IEQ_CURL_BLOCK") {
       int *b = key == "IEQ_COL_BLOCK" ? s.col_block : s.curl_block;
       char tail = 0;
@@ -141,6 +142,14 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         return false;
       }
       s.xband = std::atoi(val.c_str());
+    } else if (key == "IEQ_ZMARCH_TZ") {
+      char tail = 0;
+      int v = 0;
+      if (std::sscanf(val.c_str(), "%d%c", &v, &tail) != 1 || v < 0) {
+        err = "IEQ_ZMARCH_TZ must be a non-negative integer (0: chosen per grid)";
+        return false;
+      }
+      s.zmarch_tz = v;
     } else if (key == "IEQ_PDL") {
       if (val != "0" && val != "1") {
         err = "IEQ_PDL must be 0 or 1";

@@ -3,6 +3,7 @@
 // the instantiations compile in parallel.
 #include "stage_brick.cuh"
 #include "stage_x2.cuh"
+#include "stage_z.cuh"
 
 namespace ieq {
 
@@ -351,6 +352,45 @@ void launch_curl_brick<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, cons
                                       bool per, cudaStream_t s) {
   if (per) launch_curl_brick_p<true>(a, maps, err, s);
   else launch_curl_brick_p<false>(a, maps, err, s);
+}
+
+// the one-pass Hall stage (stage_z.cuh): dynamic shared memory above 48 KB is opted into
+// once per instantiation; resident CTAs per SM from the occupancy calculator
+template <bool HOD>
+static void launch_zmarch_h(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, const IEQ_R *rho, bool pdl, int tz_set,
+                            cudaStream_t s) {
+  constexpr int RI = Op<IEQ_OP>::RI;
+  constexpr size_t smem = ZLayout<IEQ_R, RI>::BYTES;
+  auto kern = k_stage_hall_z<IEQ_R, IEQ_OP, HOD>;
+  static int resident = 0;
+  if (resident == 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0, nsm = 0, dev = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kZThreads, smem);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    resident = per_sm * nsm > 0 ? per_sm * nsm : 1;
+  }
+  const int tz = tz_set > 0 ? (tz_set < a.m.nz ? tz_set : a.m.nz) : zm_chunk(a.m.nx, a.m.ny, a.m.nz, RI, resident);
+  const dim3 g((a.m.nx / kZTX) * (a.m.ny / kZTY), (a.m.nz + tz - 1) / tz, 1);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = dim3(kZThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, a, rho, tz);
+}
+
+template <>
+void launch_stage_zmarch<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, const IEQ_R *rho, bool hod, bool pdl,
+                                        int tz, cudaStream_t s) {
+  if (hod) launch_zmarch_h<true>(a, rho, pdl, tz, s);
+  else launch_zmarch_h<false>(a, rho, pdl, tz, s);
 }
 
 }  // namespace ieq

@@ -115,6 +115,8 @@ class Maps:
             s += f" -DIEQ_PDL={int(bool(self.I_Tech['pdl']))}"
         if self.I_Tech.get("xband") is not None:   # boxes: x boundary columns in a launch of their own
             s += f" -DIEQ_XBAND={int(self.I_Tech['xband'])}"
+        if self.I_Tech.get("zmarch_tz") is not None:   # z planes per CTA of the one-pass Hall stage
+            s += f" -DIEQ_ZMARCH_TZ={int(self.I_Tech['zmarch_tz'])}"
         return s
 
     def kernel_path_list(self) -> list[str]:

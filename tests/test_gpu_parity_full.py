@@ -34,7 +34,7 @@ import pytest
 from oracle.hostloops import clean_div, time_loop
 from oracle.sequencing import NUM_FIELDS, rk_step
 from tests.golden.cases import NOISE_AMPLITUDE, NOISE_SEED
-from tests.helpers import maps_for, own_scale_err, ref_runner_for
+from tests.helpers import field_ok, maps_for, own_scale_err, ref_runner_for, rounding_floor, stages_of
 
 pytestmark = pytest.mark.gpu
 
@@ -78,9 +78,17 @@ def _compare(ctx, c, host, dev, what):
     nf = NUM_FIELDS[c["integrator"]]
     fields = [0, 1] + ([2] if nf == 3 else []) + ([3] if c.get("hall") else [])
     names = {0: "b", 1: "b2", 2: "b3", 3: "curlB_rho"}
+    mb, mu = float(np.abs(host[0]).max()), float(np.abs(host[4]).max())
+    ns = stages_of(c, 1)
     for i in fields:
-        e = own_scale_err(ctx.get_vec(dev[i]), host[i])
-        assert e <= tol(c), (what, names[i], e)
+        # the state on its own scale at the tolerance; the RK registers (DT x DB for the 2N
+        # schemes; b2/b3 of SSPRK33 are states) and the curl buffer on their own scale plus
+        # the forward-error floor of a derivative of the state
+        reg = i == 1 and nf == 2
+        fl = rounding_floor(c, "register", mb, mu, ns) if reg else (
+            rounding_floor(c, "curl", mb, mu, ns) if i == 3 else 0.0)
+        ok, e = field_ok(ctx.get_vec(dev[i]), host[i], tol(c), fl)
+        assert ok, (what, names[i], e)
     t = ctx.get_scalar(dev[6], n=2)
     np.testing.assert_allclose(t, host[6], rtol=1e-15 if c.get("real") != "float" else 1e-6)
 
