@@ -346,6 +346,46 @@ def sharded_batch(rk, dev, steps=200, reps=3):
                        "solves_per_rank": [len(p) for p in parts], "mode": "branches"}}
 
 
+def decomposed_solve(rk, dev, n=128, steps=4, reps=3):
+    """One whistler solve (6th order + HOD, Hall, CK2N54, FP64, periodic n^3) decomposed into
+    z slabs over the ranks (inductioneq_b200.decomp: each rank runs the reference kernel lists
+    on its slab, ghost planes exchanged between kernels through NCCL); value = the solve's
+    DOF-updates / max-over-ranks time (strong scaling: the grid is fixed)."""
+    import numpy as np
+    import torch
+
+    from inductioneq_b200 import ranks as R
+    from inductioneq_b200.decomp import SlabSolve
+    dx = 2 * math.pi / n
+    m = maps(n)
+    m.I_TI.update({"DT": 0.2 * dx * dx})
+    s = SlabSolve(m, rk, dev)
+    g = m.context(device=dev)   # the initial state, made once on every rank
+    b = g.vec()
+    g.kernel("init_b", b)
+    b0 = g.get_vec(b)[: g.n]
+    g.close()
+    s.load(b0, None, np.ones(n ** 3))
+    s.steps(1)   # warm
+    times = []
+    for _ in range(reps):
+        s.load(b0, None, np.ones(n ** 3))
+        R.barrier(rk)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.steps(steps)
+        times.append(time.perf_counter() - t0)
+    t = R.max_over_ranks(rk, statistics.median(times), device="cuda")
+    s.close()
+    return {"metric": METRIC + " (one solve decomposed into z slabs)", "value": 3 * n ** 3 * STAGES * steps / t,
+            "unit": "DOF/s", "n_gpus": rk.world, "ms_per_rk_step": t / steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "dtype": "f64", "data": "synthetic (analytic whistler wave)",
+            "config": {"workload": f"hall_circular_wave {n}^3 periodic, 6th order + HOD, CK2N54, decomposed into "
+                                   f"{rk.world} z slabs", "ghost_planes": s.slabs.ghosts,
+                       "timing": "host clock around the steps (the kernels of a slab and its exchanges are "
+                                 "ordered by device synchronisation), max over ranks"}}
+
+
 def form_precision(dev, n=128, steps=20):
     """Confined-domain Hall case on 128^3: FP32 state with FP64 CG cleaning to ||r||_2 < 1e-10,
     then CK2N54 steps; compared with the FP64 run.  Reported per precision: the weighted
@@ -639,6 +679,8 @@ def main() -> None:
                     help="one node per thread in the Hall column kernels (IEQ_COL_PAIRS=0)")
     ap.add_argument("--sharded-batch", action="store_true",
                     help="only the batched form, its 32 solves split between the ranks")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="one 128^3 whistler solve decomposed into z slabs over the ranks")
     ap.add_argument("--form", default=None,
                     help="run only this form (fp32, rotation_c1, hbm_256, batched, precision_c3, adjoint_c5) "
                          "on one GPU and print its JSON")
@@ -678,6 +720,12 @@ def main() -> None:
         forms = {"rotation_c1": form_rotation40, "hbm_256": form_hbm256, "batched": form_batched,
                  "precision_c3": form_precision, "adjoint_c5": form_adjoint}
         print(json.dumps({a.form: forms[a.form](dev)}))
+        R.finish(rk)
+        return
+    if a.decomposed:
+        line = decomposed_solve(rk, dev)
+        if rank == 0:
+            print(json.dumps(line))
         R.finish(rk)
         return
     if a.sharded_batch:

@@ -57,8 +57,9 @@ typedef struct ieq_ctx ieq_ctx;
  *   and, choosing kernels of the fused time stepping without changing its results beyond
  *   the compiler's FMA contraction: -DIEQ_STAGE_KERNEL=AUTO|COLUMN|NODE|BRICK|LIST|ZMARCH
  *   (ZMARCH: the one-pass Hall stage that marches through z -- curl, E = J x B, dissipation
- *   and update in one kernel -- wherever it can run; AUTO takes it on periodic grids of at
- *   least 2^21 nodes), -DIEQ_ZMARCH_TZ=<z planes per CTA of that kernel; 0 chosen per grid>,
+ *   and update in one kernel -- wherever it can run; AUTO does not take it: it measured
+ *   slower than the curl + stage kernel pair), -DIEQ_ZMARCH_TZ=<z planes per CTA of that
+ *   kernel; 0 chosen per grid>,
  *   -DIEQ_COL_BLOCK=XxYxZ / -DIEQ_CURL_BLOCK=XxYxZ (128-thread block shapes of the column
  *   stage and curl kernels), -DIEQ_COL_PAIRS=0|1|4 (nodes per thread: one; the measured
  *   default; FP32 quads on every grid), -DIEQ_XBAND=0|1|2 (a box's x boundary columns in a
@@ -168,6 +169,14 @@ ieq_status ieq_check_finite(ieq_ctx *ctx, const void *vec_field);
  * outstanding after that second wait is reported as a different IEQ_ERR_TIMEOUT message:
  * the context's results are then undefined and it should be destroyed. */
 ieq_status ieq_test_brick_wait(ieq_ctx *ctx, int first_wait_gives_up);
+
+/* The reference kernel list of one time step of the configured integrator, as the MATLAB
+ * host builds it (compute_numerical_solution_setup.m:140-371): names separated by '\n'
+ * written to `names` (NUL-terminated; `capacity` bytes) and their number to *count.  With
+ * names == NULL only the count is returned.  Hosts that interleave their own work between
+ * the kernels of a step (the z-slab decomposition's ghost exchanges) run the list through
+ * ieq_run_kernels one name at a time. */
+ieq_status ieq_step_kernels(ieq_ctx *ctx, char *names, size_t capacity, int *count);
 
 /* Profiling (the per-kernel counterpart of the kernel time MatCL returns): every launch of
  * one ieq_time_steps step is captured alone, `repeats` times back to back, into a CUDA graph

@@ -23,8 +23,12 @@ namespace {
 
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs; fixed so that sums are reproducible
 constexpr int kMaxPartials = 65536;  // CG fused-dot partials (one per stencil block)
-// grids from which IEQ_STAGE_KERNEL=AUTO runs the one-pass Hall stage (stage_z.cuh)
-constexpr long long kZmarchAutoNodes = 1LL << 21;
+// grids from which IEQ_STAGE_KERNEL=AUTO runs the one-pass Hall stage (stage_z.cuh).
+// Measured on B200 (whistler, 6th order + HOD, FP64): 1.73 ms per stage at 256^3 against
+// 0.78 ms for the curl + stage pair (0.22 / 0.69 ms at 128^3): its shared-memory E ring
+// leaves about 23 KB of L1, the B stencil loads hit L1 33 % of the time and the kernel is
+// L2-latency bound.  AUTO therefore never takes it; IEQ_STAGE_KERNEL=ZMARCH does.
+constexpr long long kZmarchAutoNodes = 1LL << 62;
 
 #define IEQ_CUDA(ctx, call)                                                                    \
   do {                                                                                         \
@@ -59,6 +63,8 @@ Mesh mesh_of(const ieq_ctx *c) {
     m.d[a] = c->s.d[a];
   }
   m.omega = c->s.omega;
+  m.zoff = c->s.zoff;
+  m.nzg = c->s.nzg;
   return m;
 }
 

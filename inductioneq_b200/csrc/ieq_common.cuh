@@ -116,13 +116,22 @@ struct Mesh {
   double xmin[3];
   double d[3];       // DX, DY, DZ
   double omega;      // rotation rate of TC_ROTATION_GAUSSIAN
+  // a z slab of a decomposed periodic grid: local plane iz is global plane iz + zoff (modulo
+  // nzg, the global plane count) -- coordinates are those of the global grid; nzg = 0: the
+  // grid is the whole domain
+  int zoff, nzg;
 };
 
 template <typename R>
 __device__ __forceinline__ void coords(const Mesh &m, int ix, int iy, int iz, R &x, R &y, R &z) {
+  int gz = iz;
+  if (m.nzg > 0) {
+    gz = (iz + m.zoff) % m.nzg;
+    gz += gz < 0 ? m.nzg : 0;
+  }
   x = (R)m.xmin[0] + (R)ix * (R)m.d[0];
   y = (R)m.xmin[1] + (R)iy * (R)m.d[1];
-  z = (R)m.xmin[2] + (R)iz * (R)m.d[2];
+  z = (R)m.xmin[2] + (R)gz * (R)m.d[2];
 }
 
 // include/rotation_2D.h:7-25

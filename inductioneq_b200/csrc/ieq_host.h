@@ -42,7 +42,7 @@ struct Settings {
   // (the TMA brick kernels for the u = 0 stages where their rules hold, else COLUMN),
   // 4 LIST (no fusion: the reference's kernel list of each step on the caller's fields),
   // 5 ZMARCH (the one-pass Hall stage of stage_z.cuh wherever it can run, else COLUMN; AUTO
-  // takes it on grids of at least kZmarchAutoNodes nodes)
+  // takes it on grids of at least kZmarchAutoNodes nodes, which measured slower: never)
   int stage_kernel = 0;
   // thread-block shapes of the column stage kernel (IEQ_COL_BLOCK=XxYxZ) and of the curl
   // kernel (IEQ_CURL_BLOCK); X * Y * Z = 128, all zero for the default 32x4x1
@@ -59,6 +59,10 @@ struct Settings {
   int xband = 1;
   // IEQ_ZMARCH_TZ: z planes per CTA of the one-pass Hall stage (0: chosen per grid)
   int zmarch_tz = 0;
+  // IEQ_Z_OFFSET / IEQ_NZ_GLOBAL: this grid is a z slab of a decomposed periodic grid of
+  // IEQ_NZ_GLOBAL planes whose plane 0 is global plane IEQ_Z_OFFSET (testcase coordinates
+  // are the global grid's); 0 / 0: the grid is the whole domain
+  int zoff = 0, nzg = 0;
 };
 
 // parse helpers (settings.cpp)

@@ -150,6 +150,14 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         return false;
       }
       s.zmarch_tz = v;
+    } else if (key == "IEQ_Z_OFFSET" || key == "IEQ_NZ_GLOBAL") {
+      char tail = 0;
+      int v = 0;
+      if (std::sscanf(val.c_str(), "%d%c", &v, &tail) != 1 || (key == "IEQ_NZ_GLOBAL" && v < 0)) {
+        err = key + " must be an integer (IEQ_NZ_GLOBAL >= 0)";
+        return false;
+      }
+      (key == "IEQ_Z_OFFSET" ? s.zoff : s.nzg) = v;
     } else if (key == "IEQ_PDL") {
       if (val != "0" && val != "1") {
         err = "IEQ_PDL must be 0 or 1";

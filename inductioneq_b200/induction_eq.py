@@ -66,6 +66,9 @@ class Maps:
                                                     "testcase": "rotation_3D", "variable_u": False,
                                                     "periodic": "NONE"})
     tc_omega: float = 1.0
+    # (DX, DY, DZ) given instead of derived from the box (a z slab of a decomposed grid keeps
+    # the global spacing)
+    spacing_override: tuple | None = None
 
     # initialize.m:12-21
     def spacing(self) -> tuple[float, float, float]:
@@ -81,7 +84,7 @@ class Maps:
     def settings(self) -> str:
         """compute_numerical_solution_setup.m:97-137."""
         m = dict(self.I_Mesh)
-        m["DX"], m["DY"], m["DZ"] = self.spacing()
+        m["DX"], m["DY"], m["DZ"] = self.spacing_override or self.spacing()
         tech = dict(self.I_Tech)
         tech["REAL4"] = tech["REAL"] + "4"
         s = generate_settings(self.I_IEq, ["form_uibj", "form_source", "form_ujbi", "hall_term"])
@@ -117,6 +120,8 @@ class Maps:
             s += f" -DIEQ_XBAND={int(self.I_Tech['xband'])}"
         if self.I_Tech.get("zmarch_tz") is not None:   # z planes per CTA of the one-pass Hall stage
             s += f" -DIEQ_ZMARCH_TZ={int(self.I_Tech['zmarch_tz'])}"
+        if self.I_Tech.get("nz_global"):   # a z slab of a decomposed grid (inductioneq_b200.decomp)
+            s += f" -DIEQ_Z_OFFSET={int(self.I_Tech['z_offset'])} -DIEQ_NZ_GLOBAL={int(self.I_Tech['nz_global'])}"
         return s
 
     def kernel_path_list(self) -> list[str]:

@@ -87,6 +87,7 @@ def load() -> ctypes.CDLL:
     lib.ieq_compute_results.argtypes = [vp, vp, ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_double * 4)]
     lib.ieq_check_finite.argtypes = [vp, vp]
     lib.ieq_test_brick_wait.argtypes = [vp, ctypes.c_int]
+    lib.ieq_step_kernels.argtypes = [vp, ctypes.c_char_p, sz, ctypes.POINTER(ctypes.c_int)]
     lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.POINTER(KernelRecord),
                                                 ctypes.POINTER(ctypes.c_int)]
     lib.ieq_operator_jvp.argtypes = [vp] * 6
@@ -215,6 +216,14 @@ class Context:
         self._check(self.lib.ieq_run_kernels_host(self.h, nm, len(names), g, av, sz, len(arrays),
                                                   ctypes.byref(el)))
         return el.value
+
+    def step_kernels(self) -> list[str]:
+        """The reference kernel list of one time step of the configured integrator."""
+        n = ctypes.c_int(0)
+        self._check(self.lib.ieq_step_kernels(self.h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(64 * max(n.value, 1))
+        self._check(self.lib.ieq_step_kernels(self.h, buf, len(buf), ctypes.byref(n)))
+        return [k for k in buf.value.decode().split("\n") if k]
 
     def kernel(self, name: str, *args) -> None:
         """The typed entry point ieq_<name> (reference NDRange)."""

@@ -1,0 +1,162 @@
+"""The z-slab decomposition of one periodic solve (inductioneq_b200.decomp) on CPU ranks.
+
+Every rank (a spawned process, gloo) runs the integrator's kernel list on its slab with the
+oracle as the per-rank engine and exchanges the ghost planes of the state fields between
+kernels; the owned planes of every rank must equal the single-process run of the whole grid
+bit for bit (each owned node performs the same arithmetic).  Two ranks (the upper and lower
+neighbour are the same rank) and three ranks (different neighbours), Hall + high-order
+dissipation with CarpenterKennedy2N54 and Hall with a constant velocity with SSPRK33.
+"""
+from __future__ import annotations
+
+import math
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from inductioneq_b200 import decomp as D
+from inductioneq_b200 import ranks as R
+
+HP = 4.0 * math.pi / 3.0
+
+CASES = {
+    "whistler_4c_hod_ck": dict(order=4, testcase="hall_circular_wave", nodes=(8, 9, 12), lo=0.0, hi=2 * math.pi,
+                               hall=True, dissipation="HIGH_ORDER", integrator="CarpenterKennedy2N54", dt=0.01,
+                               steps=2),
+    "hallper_2c_conv_ssp": dict(order=2, testcase="hall_periodic", nodes=(7, 8, 9), lo=0.0, hi=HP, hall=True,
+                                integrator="SSPRK33", dt=0.005, steps=2),
+}
+
+
+def _oracle(c, nodes):
+    from oracle.numpy_oracle import NumpyOracle, OracleConfig
+    cfg = OracleConfig(nodes=nodes, xmin=(c["lo"],) * 3, xmax=(c["hi"],) * 3, order=c["order"], periodic=True,
+                       hall=c.get("hall", False), dissipation=c.get("dissipation", "NONE"), testcase=c["testcase"],
+                       dt=c["dt"])
+    return NumpyOracle(cfg)
+
+
+def _initial(c):
+    o = _oracle(c, c["nodes"])
+    b, u = o.vec(), o.vec()
+    o.run("init_b", o.cfg.nodes, b)
+    o.run("init_u", o.cfg.nodes, u)
+    b[:, :3] += 1e-2 * np.random.default_rng(7).standard_normal((o.N, 3))
+    return o, b, u
+
+
+def _global_run(c):
+    from oracle.hostloops import time_loop
+    from oracle.sequencing import NUM_FIELDS
+    o, b, u = _initial(c)
+    nf = NUM_FIELDS[c["integrator"]]
+    f = [b, o.vec(), o.vec(), o.vec(), u, o.scalar(fill=1.0), np.zeros(2)]
+    time_loop(o, c["integrator"], c.get("hall", False), False, c["steps"], f[0], f[1], f[2] if nf == 3 else None,
+              f[3], f[4], f[5], f[6])
+    return f
+
+
+def _rank_run(rk: R.Ranks, c: dict):
+    from oracle.sequencing import NUM_FIELDS, rk_step
+    R.init(rk, "gloo", timeout_s=60.0)
+    try:
+        g, b, u = _initial(c)
+        nx, ny, nz = c["nodes"]
+        slabs = D.ZSlabs(rk, nx, ny, nz, D.ghost_depth(c["order"]))
+        o = _oracle(c, slabs.local_nodes)
+        o.d = g.d   # the global spacing
+        nf = NUM_FIELDS[c["integrator"]]
+        lb, lu = slabs.scatter(b), slabs.scatter(u)
+        b2, b3, cb = o.vec(), o.vec(), o.vec()
+        rho, t = o.scalar(fill=1.0), np.zeros(2)
+        args = [lb, b2, b3, cb, lu, rho, t] if nf == 3 else [lb, b2, cb, lu, rho, t]
+        state = [lb, b2, b3] if nf == 3 else [lb, b2]
+        seq = rk_step(c["integrator"], c.get("hall", False), False)
+        D.decomposed_steps(slabs, o, seq, c["steps"], state, args)
+        rows = slabs.owned_rows()
+        return {"z": (slabs.z0, slabs.z1), "b": lb[rows].copy(), "b2": b2[rows].copy(),
+                "b3": b3[rows].copy() if nf == 3 else None, "t": t.copy()}
+    finally:
+        R.finish(rk)
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, case, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(world),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    try:
+        q.put((rank, _rank_run(R.Ranks.from_env(), CASES[case])))
+    except Exception as e:
+        q.put((rank, ("error", type(e).__name__, str(e)[:300])))
+
+
+def _spawn(world, case):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, case, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=30)
+    return out
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_decomposed_solve_equals_single_process_run(world, case):
+    c = CASES[case]
+    if world == 3 and c["nodes"][2] < 3 * D.ghost_depth(c["order"]):
+        pytest.skip("grid too short for three slabs of this ghost depth")
+    out = _spawn(world, case)
+    for r, v in out.items():
+        assert not (isinstance(v, tuple) and v and v[0] == "error"), v
+    ref = _global_run(c)
+    plane = c["nodes"][0] * c["nodes"][1]
+    zs = sorted(v["z"] for v in out.values())
+    assert zs[0][0] == 0 and zs[-1][1] == c["nodes"][2]
+    for v in out.values():
+        rows = slice(v["z"][0] * plane, v["z"][1] * plane)
+        np.testing.assert_array_equal(v["b"], ref[0][rows])
+        np.testing.assert_array_equal(v["b2"], ref[1][rows])
+        if v["b3"] is not None:
+            np.testing.assert_array_equal(v["b3"], ref[2][rows])
+        np.testing.assert_array_equal(v["t"], ref[6])
+
+
+def test_slab_bounds_cover_the_grid():
+    for nz, w in ((12, 2), (13, 3), (64, 8), (9, 4)):
+        b = D.slab_bounds(nz, w)
+        assert b[0][0] == 0 and b[-1][1] == nz
+        assert all(b[i][1] == b[i + 1][0] for i in range(w - 1))
+        assert max(e - s for s, e in b) - min(e - s for s, e in b) <= 1
+
+
+def test_too_many_ranks_for_the_ghost_depth_is_refused():
+    with pytest.raises(ValueError):
+        D.ZSlabs(R.Ranks(4, 0, 0), 8, 8, 12, D.ghost_depth(6))
+
+
+def test_local_maps_keep_the_global_spacing_and_offset():
+    from inductioneq_b200.induction_eq import Maps
+    m = Maps()
+    m.I_Mesh.update({"NODES_X": 16, "NODES_Y": 16, "NODES_Z": 24, "XMIN": 0.0, "XMAX": 1.0, "YMIN": 0.0, "YMAX": 1.0,
+                     "ZMIN": 0.0, "ZMAX": 3.0})
+    m.I_RunOps.update({"periodic": "USE_PERIODIC", "order": 4})
+    sl = D.ZSlabs(R.Ranks(2, 1, 1), 16, 16, 24, D.ghost_depth(4))
+    lm = D.local_maps(m, sl)
+    s = lm.settings()
+    assert f"-DNODES_Z={sl.nloc}" in s and "-DIEQ_Z_OFFSET=8" in s and "-DIEQ_NZ_GLOBAL=24" in s
+    assert f"-DDZ={3.0 / 24:.16e}" in s
+    m.I_RunOps["periodic"] = "NONE"
+    with pytest.raises(ValueError):
+        D.local_maps(m, sl)

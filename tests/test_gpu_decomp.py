@@ -1,0 +1,53 @@
+"""The z-slab decomposition on the GPU with one rank: the slab (the whole grid plus ghost
+planes refreshed by a local copy) runs the reference kernel lists through the C ABI on torch
+device buffers; its owned planes equal the undecomposed run of the same kernel lists bit for
+bit.  The variable-velocity case checks that the slab's testcase coordinates are the global
+grid's (IEQ_Z_OFFSET / IEQ_NZ_GLOBAL).  Several ranks are covered on CPU
+(tests/test_decomp_cpu.py); this run has one GPU."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from inductioneq_b200 import ranks as R
+from inductioneq_b200.decomp import SlabSolve
+from tests.helpers import maps_for
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "whistler_6c_hod_ck": dict(order=6, testcase="hall_circular_wave", nodes=(32, 16, 24), lo=0.0, hi=2 * math.pi,
+                               periodic=True, hall=True, dissipation="HIGH_ORDER",
+                               integrator="CarpenterKennedy2N54", dt=0.004),
+    "hallper_4c_varu_ssp": dict(order=4, testcase="hall_periodic", nodes=(12, 14, 16), lo=0.0, hi=4 * math.pi / 3,
+                                periodic=True, hall=True, integrator="SSPRK33", dt=0.002, variable_u=True),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_single_slab_equals_undecomposed_kernel_lists(name):
+    c = CASES[name]
+    steps = 3
+    g = maps_for(dict(c, stage_kernel="LIST")).context()
+    b, u = g.vec(), g.vec()
+    g.kernel("init_b", b)
+    g.kernel("init_u", u)
+    bh = g.get_vec(b)
+    bh[: g.n, :3] += 1e-2 * np.random.default_rng(3).standard_normal((g.n, 3))
+    uh = g.get_vec(u)
+    dev = [g.vec(bh), g.vec(), g.vec(), g.vec(), g.vec(uh), g.scalar(np.ones(g.n_pad)), g.scalar(np.zeros(2), n=2)]
+    g.time_steps(*dev, steps)
+    ref = [g.get_vec(dev[i])[: g.n] for i in range(3)]
+    t_ref = g.get_scalar(dev[6], n=2)
+    s = SlabSolve(maps_for(c), R.Ranks(1, 0, 0))
+    s.load(bh[: g.n], uh[: g.n], np.ones(g.n))
+    s.steps(steps)
+    np.testing.assert_array_equal(s.owned(s.b), ref[0])
+    np.testing.assert_array_equal(s.owned(s.b2), ref[1])
+    if s.nf == 3:
+        np.testing.assert_array_equal(s.owned(s.b3), ref[2])
+    np.testing.assert_array_equal(s.time.cpu().numpy(), t_ref)
+    s.close()
+    g.close()
