@@ -12,6 +12,7 @@
 #include "stage_brick.cuh"
 #include "stage_z.cuh"
 #include "diag.cuh"
+#include "diag_curl.cuh"
 
 namespace ieq {
 void free_brick_maps(ieq_ctx *c);   // api_fused.inc

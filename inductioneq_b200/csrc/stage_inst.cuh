@@ -4,6 +4,7 @@
 #include "stage_brick.cuh"
 #include "stage_x2.cuh"
 #include "stage_z.cuh"
+#include "diag_curl.cuh"
 
 namespace ieq {
 
@@ -391,6 +392,28 @@ void launch_stage_zmarch<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, c
                                         int tz, cudaStream_t s) {
   if (hod) launch_zmarch_h<true>(a, rho, pdl, tz, s);
   else launch_zmarch_h<false>(a, rho, pdl, tz, s);
+}
+
+template <>
+void launch_curl_e_diag<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, const DiagArgs<IEQ_R, SoA<IEQ_R>> &d,
+                                       const DiagOut &o, bool per, bool hod, dim3 g, dim3 b, bool pdl,
+                                       cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  if (per) {
+    if (hod) cudaLaunchKernelEx(&cfg, k_curl_e_diag<IEQ_R, IEQ_OP, true, true>, a, d, o);
+    else cudaLaunchKernelEx(&cfg, k_curl_e_diag<IEQ_R, IEQ_OP, true, false>, a, d, o);
+  } else {
+    if (hod) cudaLaunchKernelEx(&cfg, k_curl_e_diag<IEQ_R, IEQ_OP, false, true>, a, d, o);
+    else cudaLaunchKernelEx(&cfg, k_curl_e_diag<IEQ_R, IEQ_OP, false, false>, a, d, o);
+  }
 }
 
 }  // namespace ieq

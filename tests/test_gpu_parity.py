@@ -454,9 +454,11 @@ def _series_close(got, ref, c, o):
 
 
 @pytest.mark.parametrize("name", ["rot_gauss_4c_ssprk33", "wave_6c_hall_hod_ck2n54", "rot3d_4e_split_kcl",
-                                  "hallper_4c_ssprk104_varu", "rot_gauss_4c_ssprk33_f32"])
+                                  "hallper_4c_ssprk104_varu", "rot_gauss_4c_ssprk33_f32",
+                                  "travel_6c_hall_sat_ssprk33", "confined_6e_hall_fo_cfr"])
 def test_time_steps_integrals_match_oracle(name):
-    # the per-step series of save_integrals_over_time, collected inside the step graph
+    # the per-step series of save_integrals_over_time, collected inside the step graph (Hall
+    # steps: by the step's first curl kernel; otherwise by two launches of their own)
     z, _ = _golden()
     c = STEP_CASES[name]
     ctx = maps_for(c).context()
