@@ -519,7 +519,7 @@ def form_hbm256(dev, n=256, rk_steps=10):
     return out
 
 
-def _stage_rate(dev, n, rk_steps, kernel):
+def _stage_rate(dev, n, rk_steps, kernel, tech=None):
     import numpy as np
     import torch
 
@@ -527,6 +527,7 @@ def _stage_rate(dev, n, rk_steps, kernel):
     m = maps(n)
     m.I_TI.update({"DT": 0.2 * dx * dx})
     m.I_Tech["stage_kernel"] = kernel
+    m.I_Tech.update(tech or {})
     ctx = m.context(device=dev)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     b, b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
@@ -550,7 +551,9 @@ def _stage_rate(dev, n, rk_steps, kernel):
                            "frac": compulsory * nn / per_stage / 1e9 / peak,
                            "frac_wall": compulsory * nn * STAGES * rk_steps / el / 1e9 / peak},
            "kernels": {}}
-    own = {"curl_rho": CURL_BYTES_PER_NODE, "stage_2n_fused": 144 if kernel == "COLUMN" else compulsory}
+    hodp = (tech or {}).get("hodp", 1)
+    own = {"curl_rho": CURL_BYTES_PER_NODE if hodp else CURL_BYTES_PER_NODE - 24,
+           "stage_2n_fused": (144 if hodp else 120) if kernel != "ZMARCH" else compulsory}
     for nm, v in kernels.items():
         ms = statistics.mean(v)
         r = {"launches_per_step": len(v), "avg_ms": ms}

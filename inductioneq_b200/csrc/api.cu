@@ -30,6 +30,8 @@ constexpr int kMaxPartials = 65536;  // CG fused-dot partials (one per stencil b
 // leaves about 23 KB of L1, the B stencil loads hit L1 33 % of the time and the kernel is
 // L2-latency bound.  AUTO therefore never takes it; IEQ_STAGE_KERNEL=ZMARCH does.
 constexpr long long kZmarchAutoNodes = 1LL << 62;
+// grids from which IEQ_CURL_Z=2 (the default) runs the 2.5D curl kernel on periodic grids
+constexpr long long kCurlZAutoNodes = 1LL << 62;
 
 #define IEQ_CUDA(ctx, call)                                                                    \
   do {                                                                                         \
@@ -293,6 +295,22 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
         a.Hint[s + i + RI] += (((R)op.minv[op.nb] * (R)op.DHO.at(op.nb, s + WH - 1)) * (R)op.DHO.at(op.nb, i)) * sgn;
   }
   const bool per = c->s.periodic;
+  // the 2.5D curl kernel (stage_z.cuh) on periodic grids: forced by IEQ_CURL_Z=1, or
+  // (IEQ_CURL_Z=2, the default) from kCurlZAutoNodes nodes on
+  if (per && (c->s.curl_z == 1 || (c->s.curl_z == 2 && (long long)c->n >= kCurlZAutoNodes))) {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    const int tz = cz_chunk(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2], nsm > 0 ? nsm : 148, 4);
+    switch (c->op_id) {
+      case 0: launch_curl_e_z<R, 0>(a, hod, tz, c->s.pdl, c->stream); break;
+      case 1: launch_curl_e_z<R, 1>(a, hod, tz, c->s.pdl, c->stream); break;
+      case 2: launch_curl_e_z<R, 2>(a, hod, tz, c->s.pdl, c->stream); break;
+      case 3: launch_curl_e_z<R, 3>(a, hod, tz, c->s.pdl, c->stream); break;
+      case 4: launch_curl_e_z<R, 4>(a, hod, tz, c->s.pdl, c->stream); break;
+      case 5: launch_curl_e_z<R, 5>(a, hod, tz, c->s.pdl, c->stream); break;
+    }
+    return;
+  }
   const ColShape sh = col_shape(c->s.curl_block, c->s.col_pairs, c->s.pdl, c->s.xband);
   switch (c->op_id) {
     case 0: launch_curl_e<R, 0>(a, per, hod, sh, c->stream); break;

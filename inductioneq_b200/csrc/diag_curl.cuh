@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(kColThreads) k_curl_e_diag(const __grid_consta
       stf(a.jface, idx, J);
     diag_terms(d, idx, acc[0], acc[1], acc[2]);
   }
-  // block partials, then the last block adds them in a fixed order
+  // block partials (whole warps: the launcher gives 128-thread blocks), then the last block
+  // adds them in a fixed order
   __shared__ double sm[3][kColThreads / 32];
   __shared__ bool last;
   const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);

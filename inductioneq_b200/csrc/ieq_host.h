@@ -63,6 +63,17 @@ struct Settings {
   // IEQ_NZ_GLOBAL planes whose plane 0 is global plane IEQ_Z_OFFSET (testcase coordinates
   // are the global grid's); 0 / 0: the grid is the whole domain
   int zoff = 0, nzg = 0;
+  // IEQ_CG_PASS_A: the CG's pass A as the 2.5D kernel (2, the default) or the per-node gather (1)
+  int cg_passes = 2;
+  // IEQ_CG_LOOP=HOST (profiling): the CG iterations as max_iterations launches in sequence
+  // instead of a graph loop node (kernels inside a loop node are invisible to the profiler)
+  bool cg_host_loop = false;
+  // IEQ_HODP: Hall + high-order dissipation -- 1 the curl kernel forms the dissipation sum and
+  // the stage kernel reads it; 0 the stage kernel gathers the dissipation rows itself
+  int hodp = 1;
+  // IEQ_CURL_Z: the curl kernel of periodic Hall stages as the 2.5D z march (stage_z.cuh):
+  // 0 never, 1 always, 2 (default) on grids of at least kCurlZAutoNodes nodes
+  int curl_z = 2;
 };
 
 // parse helpers (settings.cpp)

@@ -552,6 +552,7 @@ __device__ __forceinline__ double laplace_dir_at(const LapArgs<double> &a, const
 template <int W>
 __global__ void __launch_bounds__(256) k_cg_pass_a(const LapArgs<double> a, const LapFastArgs<W> f, const double *r,
                                                    double *u0, double *u1, CgState *cs, unsigned *counter) {
+  if (cs->done) return;   // (host-driven iterations past convergence)
   const int it = cs->it;
   const double *uo = (it & 1) ? u1 : u0;
   double *un = (it & 1) ? u0 : u1;
@@ -578,13 +579,118 @@ __global__ void __launch_bounds__(256) k_cg_pass_a(const LapArgs<double> a, cons
   }
 }
 
+// Pass A as a 2.5D kernel: a CTA of kCgTX x kCgTY threads owns a tile of x-y columns of the
+// CG interior and marches through a chunk of z planes.  Every thread keeps the direction
+// values of its column at planes z - C0 .. z + C0 in a register queue (the z terms), and the
+// plane z of the tile with its x and y halos (C0 deep) sits in shared memory (the x and y
+// terms), so each direction value is formed (__fma_rn(beta, u, r)) and loaded from global
+// memory about once per node instead of once per stencil point.  Values outside the grid are
+// 0 (their coefficient is 0, where the reference reads the node itself); periodic grids wrap.
+// The terms are summed in the order of laplace_dir_at: per row entry c, ((val + x) + y) + z.
+constexpr int kCgTX = 32, kCgTY = 8;
+
+// the direction value at global node (x, y, z): 0 outside the grid (non-periodic)
+__device__ __forceinline__ double cg_dir_at(const LapArgs<double> &a, const double *uo, const double *r, double beta,
+                                            int x, int y, int z) {
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  if (a.periodic) {
+    x += x < 0 ? nx : 0; x -= x >= nx ? nx : 0;
+    y += y < 0 ? ny : 0; y -= y >= ny ? ny : 0;
+    z += z < 0 ? nz : 0; z -= z >= nz ? nz : 0;
+  } else if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) {
+    return 0.0;
+  }
+  const long long j = x + (long long)nx * (y + (long long)ny * z);
+  return __fma_rn(beta, __ldg(uo + j), __ldg(r + j));
+}
+
+template <int W>
+__global__ void __launch_bounds__(kCgTX * kCgTY) k_cg_pass_a_z(const LapArgs<double> a, const LapFastArgs<W> f,
+                                                                const double *r, double *u0, double *u1, CgState *cs,
+                                                                unsigned *counter, int tz) {
+  if (cs->done) return;   // (host-driven iterations past convergence)
+  constexpr int C0 = (W - 1) / 2;
+  constexpr int SX = kCgTX + 2 * C0, SY = kCgTY + 2 * C0;
+  __shared__ double pl[SY][SX];
+  const int it = cs->it;
+  const double *uo = (it & 1) ? u1 : u0;
+  double *un = (it & 1) ? u0 : u1;
+  const double beta = cs->rr / cs->old;
+  const int tx = threadIdx.x % kCgTX, ty = threadIdx.x / kCgTX;
+  const int x0 = a.off + blockIdx.x * kCgTX, y0 = a.off + blockIdx.y * kCgTY;
+  const int zb = a.off + blockIdx.z * tz;
+  const int ze = min(zb + tz, a.off + a.gz);
+  const int ix = x0 + tx, iy = y0 + ty;
+  const bool mine = ix < a.off + a.gx && iy < a.off + a.gy;
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int rows = 2 * a.nb + 1;
+  const int rx = a.periodic ? a.nb : sbp_row(ix, nx, a.nb);
+  const int ry = a.periodic ? a.nb : sbp_row(iy, ny, a.nb);
+  const double *lx = f.Ls + ((long long)0 * rows + rx) * W;
+  const double *ly = f.Ls + ((long long)1 * rows + ry) * W;
+  double q[W];
+#pragma unroll
+  for (int k = 0; k < W - 1; ++k) q[k + 1] = mine ? cg_dir_at(a, uo, r, beta, ix, iy, zb - C0 + k) : 0.0;
+  double prod = 0.0;
+  for (int z = zb; z < ze; ++z) {
+#pragma unroll
+    for (int k = 0; k < W - 1; ++k) q[k] = q[k + 1];
+    q[W - 1] = mine ? cg_dir_at(a, uo, r, beta, ix, iy, z + C0) : 0.0;
+    // the tile of plane z (own column: the queue centre) and its x / y halos
+    // (a thread past the interior holds the value of its own grid position: 0 on a box, the
+    // wrapped value on a periodic grid)
+    pl[ty + C0][tx + C0] = mine ? q[C0] : cg_dir_at(a, uo, r, beta, ix, iy, z);
+    for (int h = threadIdx.x; h < 2 * C0 * kCgTY + 2 * C0 * kCgTX; h += kCgTX * kCgTY) {
+      int px, py;
+      if (h < 2 * C0 * kCgTY) {   // x halo: C0 columns on each side of every tile row
+        const int side = h / (C0 * kCgTY), rem = h % (C0 * kCgTY);
+        py = C0 + rem / C0;
+        px = side ? kCgTX + C0 + rem % C0 : rem % C0;
+      } else {                     // y halo: C0 rows above and below the tile's columns
+        const int g = h - 2 * C0 * kCgTY;
+        const int side = g / (C0 * kCgTX), rem = g % (C0 * kCgTX);
+        px = C0 + rem % kCgTX;
+        py = side ? kCgTY + C0 + rem / kCgTX : rem / kCgTX;
+      }
+      pl[py][px] = cg_dir_at(a, uo, r, beta, x0 - C0 + px, y0 - C0 + py, z);
+    }
+    __syncthreads();
+    if (mine) {
+      const int rz = a.periodic ? a.nb : sbp_row(z, nz, a.nb);
+      const double *lz = f.Ls + ((long long)2 * rows + rz) * W;
+      double val = 0.0;
+#pragma unroll
+      for (int c = 0; c < W; ++c) {
+        const double t0 = pl[ty + C0][tx + c] * lx[c];
+        const double t1 = pl[ty + c][tx + C0] * ly[c];
+        const double t2 = q[c] * lz[c];
+        val = ((val + t0) + t1) + t2;
+      }
+      const long long idx = ix + (long long)nx * (iy + (long long)ny * z);
+      un[idx] = q[C0];
+      a.out[idx] = val;
+      prod += q[C0] * val;
+    }
+    __syncthreads();
+  }
+  if (block_partial_and_ticket(prod, a.partials, counter)) {
+    const int np = gridDim.x * gridDim.y * gridDim.z;
+    const double ul = block_sum_partials(a.partials, np);
+    if (threadIdx.x == 0) {
+      cs->alpha = cs->rr / ul;
+      *counter = 0u;
+    }
+  }
+}
+
 // Pass B (clean_div.m:57-66): phi += alpha*u (calc_xpay), r -= alpha*lap, rr = <r, r> (last
 // block), then the loop condition of clean_div.m:47, written to the graph loop's condition
 template <typename S>
 __global__ void __launch_bounds__(256) k_cg_pass_b(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,
                                                    const S *u0, const S *u1, const S *lap, double *partials,
                                                    CgState *cs, unsigned *counter, double *history,
-                                                   cudaGraphConditionalHandle loop) {
+                                                   cudaGraphConditionalHandle loop, int in_loop) {
+  if (cs->done) return;                  // (host-driven iterations past convergence)
   const S *u = (cs->it & 1) ? u0 : u1;   // the direction pass A of this iteration wrote
   const S alpha = (S)cs->alpha;
   const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
@@ -607,7 +713,7 @@ __global__ void __launch_bounds__(256) k_cg_pass_b(Mesh m, int off, int gx, int 
       cs->it += 1;
       if (history) history[cs->it] = tot;
       cs->done = !(tot > cs->tol && cs->it < cs->max_it);
-      cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
+      if (in_loop) cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
       *counter = 0u;
     }
   }
@@ -627,7 +733,7 @@ static __global__ void k_cg_init(CgState *cs, double tol, int max_it) {
 // initial residual r = div B: rr = <r, r> from reduction partials, the loop condition, and
 // the graph loop's condition (no iteration when the field is already clean)
 static __global__ void k_cg_start_loop(const double *partials_rr, int np, CgState *cs, double *history,
-                                       cudaGraphConditionalHandle loop) {
+                                       cudaGraphConditionalHandle loop, int in_loop) {
   const double rr = block_sum_partials(partials_rr, np);
   if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
     cs->rr = rr;
@@ -635,7 +741,7 @@ static __global__ void k_cg_start_loop(const double *partials_rr, int np, CgStat
     cs->it = 0;
     if (history) history[0] = rr;
     cs->done = !(rr > cs->tol && cs->it < cs->max_it);
-    cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
+    if (in_loop) cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
   }
 }
 

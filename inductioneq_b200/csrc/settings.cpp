@@ -158,6 +158,30 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         return false;
       }
       (key == "IEQ_Z_OFFSET" ? s.zoff : s.nzg) = v;
+    } else if (key == "IEQ_CG_LOOP") {
+      if (val != "GRAPH" && val != "HOST") {
+        err = "IEQ_CG_LOOP must be GRAPH or HOST";
+        return false;
+      }
+      s.cg_host_loop = val == "HOST";
+    } else if (key == "IEQ_CURL_Z") {
+      if (val != "0" && val != "1" && val != "2") {
+        err = "IEQ_CURL_Z must be 0, 1 or 2";
+        return false;
+      }
+      s.curl_z = std::atoi(val.c_str());
+    } else if (key == "IEQ_HODP") {
+      if (val != "0" && val != "1") {
+        err = "IEQ_HODP must be 0 or 1";
+        return false;
+      }
+      s.hodp = std::atoi(val.c_str());
+    } else if (key == "IEQ_CG_PASS_A") {
+      if (val != "1" && val != "2") {
+        err = "IEQ_CG_PASS_A must be 1 (per-node gather) or 2 (2.5D z march)";
+        return false;
+      }
+      s.cg_passes = std::atoi(val.c_str());
     } else if (key == "IEQ_PDL") {
       if (val != "0" && val != "1") {
         err = "IEQ_PDL must be 0 or 1";

@@ -59,8 +59,8 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-template <typename Kern, typename Arg>
-inline void launch_pdl(Kern kernel, dim3 grid, dim3 block, cudaStream_t s, bool pdl, const Arg &a) {
+template <typename Kern, typename... Args>
+inline void launch_pdl(Kern kernel, dim3 grid, dim3 block, cudaStream_t s, bool pdl, const Args &...a) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -71,7 +71,7 @@ inline void launch_pdl(Kern kernel, dim3 grid, dim3 block, cudaStream_t s, bool 
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, kernel, a);
+  cudaLaunchKernelEx(&cfg, kernel, a...);
 }
 
 template <typename R>

@@ -416,4 +416,11 @@ void launch_curl_e_diag<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, con
   }
 }
 
+template <>
+void launch_curl_e_z<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int tz, bool pdl, cudaStream_t s) {
+  const dim3 g((a.m.nx + kCzTX - 1) / kCzTX, (a.m.ny + kCzTY - 1) / kCzTY, (a.m.nz + tz - 1) / tz);
+  if (hod) launch_pdl(k_curl_e_z<IEQ_R, IEQ_OP, true>, g, dim3(kCzTX * kCzTY), s, pdl, a, tz);
+  else launch_pdl(k_curl_e_z<IEQ_R, IEQ_OP, false>, g, dim3(kCzTX * kCzTY), s, pdl, a, tz);
+}
+
 }  // namespace ieq

@@ -376,3 +376,127 @@ inline int zm_chunk(int nx, int ny, int nz, int ri, int resident) {
 }
 
 }  // namespace ieq
+
+namespace ieq {
+
+// ---------------------------------------------------------------------------------------
+// The curl kernel as a 2.5D z march (periodic grids): J = curl(B)/rho, E = J x B and (HODS)
+// the dissipation sum of B, the outputs of k_curl_e_x2 / k_curl_e_hod, with each value of B
+// loaded from global memory about once.  A CTA of kCzTX x kCzTY threads owns a tile of x-y
+// columns and a chunk of z planes; every thread keeps the three components of B of its
+// column at planes z - RI .. z + RI in registers (the z terms) and plane z of the tile with
+// its x and y halos (RI deep) sits in shared memory (the x and y terms).  The sums run in the
+// order of k_curl_e_hod (axis by axis, offsets ascending), so the outputs equal the one-node
+// kernels' up to the compiler's fused multiply-adds.
+constexpr int kCzTX = 32, kCzTY = 8;
+
+template <typename R, int OP, bool HODS>
+__global__ void __launch_bounds__(kCzTX * kCzTY) k_curl_e_z(const __grid_constant__ CurlArgs<R, SoA<R>> a, int tz) {
+  constexpr int RI = Op<OP>::RI, W = 2 * RI + 1;
+  constexpr int SX = kCzTX + 2 * RI, SY = kCzTY + 2 * RI;
+  __shared__ R pl[3][SY][SX];
+  pdl_enter();
+  const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
+  const int tx = threadIdx.x % kCzTX, ty = threadIdx.x / kCzTX;
+  const int x0 = blockIdx.x * kCzTX, y0 = blockIdx.y * kCzTY;
+  const int zb = blockIdx.z * tz, ze = min(zb + tz, nz);
+  const int ix = x0 + tx, iy = y0 + ty;
+  const long long sz = (long long)nx * ny;
+  const long long cs = a.b.s;
+  auto wrap = [](int i, int n) { i %= n; return i < 0 ? i + n : i; };
+  // the column of (ix, iy) wrapped into the grid (threads past the edge hold the periodic image)
+  const long long col = wrap(ix, nx) + (long long)nx * wrap(iy, ny);
+  R q[3][W];
+#pragma unroll
+  for (int k = 0; k < W - 1; ++k) {
+    const long long j = col + sz * wrap(zb - RI + k, nz);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) q[c][k + 1] = __ldg(a.b.p + j + c * cs);
+  }
+  for (int z = zb; z < ze; ++z) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) q[c][k] = q[c][k + 1];
+      q[c][W - 1] = __ldg(a.b.p + col + sz * wrap(z + RI, nz) + c * cs);
+      pl[c][ty + RI][tx + RI] = q[c][RI];
+    }
+    // halos of plane z: RI columns left and right of every tile row, RI rows above and below
+    for (int h = threadIdx.x; h < 2 * RI * kCzTY + 2 * RI * kCzTX; h += kCzTX * kCzTY) {
+      int px, py;
+      if (h < 2 * RI * kCzTY) {
+        const int side = h / (RI * kCzTY), rem = h % (RI * kCzTY);
+        py = RI + rem / RI;
+        px = side ? kCzTX + RI + rem % RI : rem % RI;
+      } else {
+        const int g = h - 2 * RI * kCzTY;
+        const int side = g / (RI * kCzTX), rem = g % (RI * kCzTX);
+        px = RI + rem % kCzTX;
+        py = side ? kCzTY + RI + rem / kCzTX : rem / kCzTX;
+      }
+      const long long j = wrap(x0 - RI + px, nx) + (long long)nx * wrap(y0 - RI + py, ny) + sz * z;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pl[c][py][px] = __ldg(a.b.p + j + c * cs);
+    }
+    __syncthreads();
+    if (ix < nx && iy < ny) {
+      const V3<R> Bm = {q[0][RI], q[1][RI], q[2][RI]};
+      R g[3][3];
+      V3<R> hod = {0, 0, 0};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+        R v1 = 0, v2 = 0;
+        V3<R> ho = {0, 0, 0};
+#pragma unroll
+        for (int o = -RI; o <= RI; ++o) {
+          // the three components of B at offset o along the axis
+          R b3[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            b3[c] = ax == 0 ? pl[c][ty + RI][tx + RI + o] : (ax == 1 ? pl[c][ty + RI + o][tx + RI] : q[c][RI + o]);
+          const R cH = a.Hint[o + RI];
+          if (o == 0) {
+            if (HODS) {
+              ho.x += cH * Bm.x; ho.y += cH * Bm.y; ho.z += cH * Bm.z;
+            }
+            continue;
+          }
+          const R cD = a.Dint[o + RI];
+          v1 += cD * b3[c1];
+          v2 += cD * b3[c2];
+          if (HODS) {
+            ho.x += cH * b3[0]; ho.y += cH * b3[1]; ho.z += cH * b3[2];
+          }
+        }
+        g[ax][c1] = v1 * a.inv_d[ax];
+        g[ax][c2] = v2 * a.inv_d[ax];
+        if (HODS) {
+          hod.x += ho.x; hod.y += ho.y; hod.z += ho.z;
+        }
+      }
+      const long long idx = ix + (long long)nx * iy + sz * z;
+      V3<R> J = {g[1][2] - g[2][1], g[2][0] - g[0][2], g[0][1] - g[1][0]};
+      if (a.rho) {
+        const R r = (R)1 / __ldg(a.rho + idx);
+        J = {J.x * r, J.y * r, J.z * r};
+      }
+      stf(a.out, idx, V3<R>{J.x * Bm.y - J.y * Bm.x, J.x * Bm.z - J.z * Bm.x, J.y * Bm.z - J.z * Bm.y});
+      if (HODS) stf(a.hout, idx, hod);
+    }
+    __syncthreads();
+  }
+}
+
+// z planes per CTA of k_curl_e_z: about `per_sm` CTAs per SM, at least 4 planes
+inline int cz_chunk(int nx, int ny, int nz, int nsm, int per_sm) {
+  const long long tiles = (long long)((nx + kCzTX - 1) / kCzTX) * ((ny + kCzTY - 1) / kCzTY);
+  const long long chunks = ((long long)per_sm * nsm + tiles - 1) / tiles;
+  int tz = (int)((nz + chunks - 1) / chunks);
+  return tz < 4 ? 4 : tz;
+}
+
+template <typename R, int OP>
+void launch_curl_e_z(const CurlArgs<R, SoA<R>> &a, bool hod, int tz, bool pdl, cudaStream_t s);
+
+}  // namespace ieq

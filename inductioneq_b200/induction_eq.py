@@ -120,6 +120,14 @@ class Maps:
             s += f" -DIEQ_XBAND={int(self.I_Tech['xband'])}"
         if self.I_Tech.get("zmarch_tz") is not None:   # z planes per CTA of the one-pass Hall stage
             s += f" -DIEQ_ZMARCH_TZ={int(self.I_Tech['zmarch_tz'])}"
+        if self.I_Tech.get("cg_loop"):   # GRAPH (default) or HOST: the CG iterations as a graph loop or host launches
+            s += f" -DIEQ_CG_LOOP={self.I_Tech['cg_loop']}"
+        if self.I_Tech.get("curl_z") is not None:   # the 2.5D curl kernel on periodic grids: 0 never, 1 always, 2 auto
+            s += f" -DIEQ_CURL_Z={int(self.I_Tech['curl_z'])}"
+        if self.I_Tech.get("hodp") is not None:   # the dissipation sum formed by the curl kernel (1) or the stage kernel (0)
+            s += f" -DIEQ_HODP={int(self.I_Tech['hodp'])}"
+        if self.I_Tech.get("cg_pass_a") is not None:   # the CG's pass A: 2 the 2.5D kernel, 1 per-node gathers
+            s += f" -DIEQ_CG_PASS_A={int(self.I_Tech['cg_pass_a'])}"
         if self.I_Tech.get("nz_global"):   # a z slab of a decomposed grid (inductioneq_b200.decomp)
             s += f" -DIEQ_Z_OFFSET={int(self.I_Tech['z_offset'])} -DIEQ_NZ_GLOBAL={int(self.I_Tech['nz_global'])}"
         return s

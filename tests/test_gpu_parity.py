@@ -636,3 +636,50 @@ def test_box_x_band_equals_pair_kernels_alone(case):
         assert ok, (i, e)
     np.testing.assert_array_equal(out[0][2], out[1][2])    # time bookkeeping by the band kernel
     assert np.isfinite(out[1][0]).all()
+
+
+@pytest.mark.parametrize("case", ["box_4c_wsd0", "box_6e_wsd0", "box_2c_wsln", "periodic_4c_wsd0"])
+def test_cg_pass_a_forms_agree(case):
+    # the CG's pass A as the 2.5D z march (default) and as per-node gathers: the same
+    # Laplacian values per node; the dot products' block partials differ, so the fields agree
+    # to the CG parity tolerance with the same iteration count (ragged tiles: 37 x 21 x 30)
+    order = int(case.split("_")[1][0])
+    c = dict(order=order, extended=case.split("_")[1].endswith("e"), testcase="confined_domain", nodes=(37, 21, 30),
+             lo=0.0, hi=1.0, laplace={"wsd0": "WIDE_STENCIL_DIRICHLET", "wsln": "WIDE_STENCIL_LNS"}[case.split("_")[2]],
+             bnodes=0 if case.endswith("wsln") else 1, periodic=case.startswith("periodic"))
+    out = []
+    for form in (2, 1):
+        ctx = maps_for(dict(c, cg_pass_a=form)).context()
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b)
+        bh[: ctx.n, :3] += NOISE_AMPLITUDE * np.random.default_rng(NOISE_SEED).random((ctx.n, 3))
+        db = ctx.vec(bh)
+        res = ctx.clean_div(db, 30, 1e-13, check=False)
+        out.append((res["iterations"], res["residual_norm2"], ctx.get_vec(db)))
+        ctx.close()
+    assert out[0][0] == out[1][0]
+    assert abs(out[0][1] - out[1][1]) <= 1e-6 * out[1][1]
+    assert rel_err(out[0][2], out[1][2]) <= 1e-11
+
+
+def test_cg_host_loop_equals_graph_loop():
+    # IEQ_CG_LOOP=HOST (the profiling form: the iterations launched one after another) runs the
+    # same kernels in the same order as the graph loop node: identical fields and counts
+    c = dict(order=4, testcase="confined_domain", nodes=(20, 18, 22), lo=0.0, hi=1.0,
+             laplace="WIDE_STENCIL_DIRICHLET", bnodes=1)
+    out = []
+    for loop in ("GRAPH", "HOST"):
+        m = maps_for(c)
+        m.I_Tech["cg_loop"] = loop
+        ctx = m.context()
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b)
+        bh[: ctx.n, :3] += NOISE_AMPLITUDE * np.random.default_rng(NOISE_SEED).random((ctx.n, 3))
+        db = ctx.vec(bh)
+        res = ctx.clean_div(db, 25, 1e-9, check=False)
+        out.append((res["iterations"], res["residual_norm2"], ctx.get_vec(db)))
+        ctx.close()
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    np.testing.assert_array_equal(out[0][2], out[1][2])

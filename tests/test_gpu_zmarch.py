@@ -1,6 +1,7 @@
-"""The one-pass Hall stage (stage_z.cuh: curl, E = J x B, dissipation and update in one kernel
-that marches through z) against the two-kernel column path, the reference kernel lists and
-the oracle.
+"""The z-marching kernels of stage_z.cuh -- the one-pass Hall stage (curl, E = J x B,
+dissipation and update in one kernel) and the 2.5D curl kernel -- against the two-kernel
+column path, the reference kernel lists and the oracle; and the dissipation sum formed in
+the stage kernel (IEQ_HODP=0) against the curl kernel's.
 
 IEQ_STAGE_KERNEL=ZMARCH forces it on grids where it can run (periodic, nx a multiple of 32,
 ny of 16); IEQ_ZMARCH_TZ sets the z planes per CTA (1: every CTA a single plane after a
@@ -118,3 +119,26 @@ def test_zmarch_matches_oracle(real):
         assert ok, (i, e)
     np.testing.assert_allclose(ctx.get_scalar(dev[6], n=2), host[6], rtol=1e-15 if real == "double" else 1e-6)
     ctx.close()
+
+
+@pytest.mark.parametrize("order, extended", [(2, False), (4, False), (6, False), (6, True)])
+@pytest.mark.parametrize("hod", [True, False])
+@pytest.mark.parametrize("real", ["double", "float"])
+def test_curl_z_march_equals_pair_curl_kernel(order, extended, hod, real):
+    # the 2.5D curl kernel (IEQ_CURL_Z=1) against the pair curl kernel (IEQ_CURL_Z=0) on a
+    # periodic grid with partial tiles in x and y (36 x 20 x 17): the same sums per node
+    c = _case(order, extended, hod, nodes=(36, 20, 17), real=real)
+    out = []
+    for cz in (1, 0):
+        out.append(_run(dict(c, curl_z=cz), "COLUMN", 3))
+    _same(c, out[0], out[1], 3, 1e-13 if real == "double" else 2e-6)
+
+
+@pytest.mark.parametrize("hodp", [0, 1])
+def test_dissipation_sum_in_stage_or_curl_kernel_agree(hodp):
+    # IEQ_HODP=0: the stage kernel gathers the dissipation rows itself instead of reading the
+    # curl kernel's sum; the same terms per node
+    c = _case(6, False, True, nodes=(32, 18, 20))
+    a = _run(dict(c, hodp=hodp), "COLUMN", 3)
+    b = _run(dict(c, hodp=1), "COLUMN", 3)
+    _same(c, a, b, 3, 1e-13)
