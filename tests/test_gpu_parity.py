@@ -468,10 +468,11 @@ def test_time_steps_integrals_match_oracle(name):
     got = ctx.time_steps_integrals(*dev, steps)
     ref = _oracle_series(o, c, host, steps)
     _series_close(got, ref, c, o)
-    # the diagnostics do not change the stepping
+    # the diagnostics do not change the stepping (Hall steps: the step's first curl kernel is
+    # the one-node diagnostic form, equal to the other curl kernels up to FMA contraction)
     _, dev2 = _fields(ctx, o, z, name)
     ctx.time_steps(*dev2, steps)
-    np.testing.assert_array_equal(ctx.get_vec(dev[0]), ctx.get_vec(dev2[0]))
+    assert rel_err(ctx.get_vec(dev[0]), ctx.get_vec(dev2[0])) <= (1e-6 if c.get("real") == "float" else 1e-13)
     np.testing.assert_array_equal(ctx.get_scalar(dev[6], n=2), ctx.get_scalar(dev2[6], n=2))
 
 
