@@ -923,6 +923,23 @@ def main() -> None:
                 out["forms"][name] = fn(dev)
             except Exception as e:
                 out["forms"][name] = {"error": repr(e)}
+    hb = out.get("forms", {}).get("hbm_256", {}).get("column")
+    if isinstance(hb, dict) and "whole_stage" in hb:
+        # the same kernels where every field is HBM resident: the whole stage at the stage's
+        # compulsory bytes, and each kernel at its own traffic (DRAM bytes per launch from the
+        # ncu summary of that size)
+        rec = {"grid": [256] * 3, "whole_stage_frac": hb["whole_stage"]["frac"],
+               "whole_stage_bytes_per_node": hb["whole_stage"]["bytes_per_node"],
+               "stage_kernel_frac": hb["kernels"].get("stage_2n_fused", {}).get("frac"),
+               "curl_kernel_frac": hb["kernels"].get("curl_rho", {}).get("frac"), "peak": peak,
+               "peak_source": peak_src}
+        summ = os.path.join(ROOT, "profiles", "hbm_stage_kernels_hall6_256cubed.md")
+        if os.path.isfile(summ):
+            with open(summ) as f:
+                for line in f:
+                    if line.startswith("traffic_bytes_per_launch"):
+                        rec["stage_kernel_traffic_per_launch"] = int(line.split(":", 1)[1].split()[0])
+        roofline["hbm_resident"] = rec
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         ref = cpu_reference_run(10 ** 6, 1, budget_s=15.0)
         one = cpu_reference_run(10 ** 6, 1, budget_s=4.0, threads=1)
