@@ -248,9 +248,11 @@ ieq_status ieq_operator_vjp(ieq_ctx *ctx, const void *b, const void *w, const vo
  * -DIEQ_VARIABLE_U=1, else the given u) */
 ieq_status ieq_ssprk33_step_vjp(ieq_ctx *ctx, const void *s1, const void *s2, const void *s3, double t0,
                                 void *lambda, const void *u, const void *rho);
-/* Gradient through num_steps SSPRK33 steps from b0 at t = 0: lambda holds dL/db(T) on entry
- * and dL/db0 on return.  The forward run is checkpointed every checkpoint_every steps and
- * each segment recomputed (stage states kept) during the reverse sweep. */
+/* Gradient through num_steps steps of the configured integrator -- SSPRK33 or one of the 2N
+ * low-storage schemes CarpenterKennedy2N54 / ToulorgeDesmet2N84F -- from b0 at t = 0: lambda
+ * holds dL/db(T) on entry and dL/db0 on return.  The forward run is checkpointed every
+ * checkpoint_every steps and each segment recomputed (stage states kept) during the reverse
+ * sweep; a 2N step is reversed stage by stage (mu2 += B_s mu1, mu1 += h F'^T mu2, mu2 = A_s mu2). */
 ieq_status ieq_adjoint_steps(ieq_ctx *ctx, const void *b0, void *lambda, const void *u, const void *rho,
                              int num_steps, int checkpoint_every);
 

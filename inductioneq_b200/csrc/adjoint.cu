@@ -282,6 +282,7 @@ namespace ieq {
 // from api.cu
 ieq_status adj_run_kernel(ieq_ctx *c, const char *name, void *const *args, int nargs);
 void adj_curl(ieq_ctx *c, const void *b, const void *rho, void *out);
+void rk2n_coefficients(bool ck, const double **A, const double **B, const double **C, int *stages);
 void adj_context(ieq_ctx *c, Mesh &m, const Tables<double> *&tab, double w[6], double inv_d[3], double two_inv_d[3],
                  double sat_s[3]);
 
@@ -421,6 +422,33 @@ ieq_status ssprk33_step_vjp_ws(ieq_ctx *c, const void *s1, const void *s2, const
   return IEQ_OK;
 }
 
+// lambda <- (d step / d b_n)^T lambda for one step of a 2N low-storage scheme
+// (kernel_time_integrator.cl:1023-1206 CarpenterKennedy2N54, 1216-1516 ToulorgeDesmet2N84F)
+// from the stage inputs x[s] (b1 before stage s) of a step that started at t0:
+//   stage s:  b2 = A_s b2 + h F(x[s], t_s);  b1 = x[s] + B_s b2    (t_0 = t0, t_s = t0 + C_{s-1} h)
+// reversed with mu1 = lambda (b1 after the step) and mu2 = 0 (the next step's first stage has
+// A_0 = 0, so b2 after a step does not reach the next):
+//   mu2 += B_s mu1;  mu1 += h F'(x[s], t_s)^T mu2;  mu2 = A_s mu2      (s = S-1 .. 0)
+// w.f[3] holds mu2; no allocation, no synchronisation
+ieq_status rk2n_step_vjp_ws(ieq_ctx *c, bool ck, void *const *x, double t0, void *lambda, const void *u,
+                            const void *rho, const VjpWork &w) {
+  void *J0 = w.f[0], *gJr = w.f[1], *z = w.f[2], *mu2 = w.f[3], *uw = w.f[6];
+  const double *A, *B, *C;
+  int S;
+  rk2n_coefficients(ck, &A, &B, &C, &S);
+  const double h = c->s.dt;
+  cudaMemsetAsync(mu2, 0, c->n_pad * sizeof(R4<double>), c->stream);
+  ieq_status st;
+  for (int s = S - 1; s >= 0; --s) {
+    const double ts = s == 0 ? t0 : t0 + C[s - 1] * h;
+    lincomb(c, mu2, 1.0, mu2, B[s], lambda);
+    if ((st = vjp(c, x[s], mu2, stage_u(c, u, uw, w.d_time, ts), rho, z, J0, gJr)) != IEQ_OK) return st;
+    lincomb(c, lambda, 1.0, lambda, h, z);
+    lincomb(c, mu2, A[s], mu2, 0.0, nullptr);
+  }
+  return IEQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -510,58 +538,83 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   if (!c || !b0 || !lambda || !u || !rho || num_steps < 0 || checkpoint_every < 1) return IEQ_ERR_ARG;
   ieq_status st = check_adjoint_settings(c);
   if (st != IEQ_OK) return st;
-  if (c->s.integrator != "SSPRK33") return afail(c, IEQ_ERR_SETTINGS, "the adjoint time stepping is SSPRK33");
+  const bool ssp = c->s.integrator == "SSPRK33";
+  const bool ck2n = c->s.integrator == "CarpenterKennedy2N54", td2n = c->s.integrator == "ToulorgeDesmet2N84F";
+  if (!ssp && !ck2n && !td2n)
+    return afail(c, IEQ_ERR_SETTINGS,
+                 "the adjoint time stepping is SSPRK33, CarpenterKennedy2N54 or ToulorgeDesmet2N84F");
   cudaSetDevice(c->device);
   const size_t vb = c->n_pad * sizeof(R4<double>);
   const int K = checkpoint_every;
   const int nseg = (num_steps + K - 1) / K;
-  // checkpoints (nseg), the stage states of one segment (3K), step work (5), step-adjoint work (7)
+  // states kept per step: SSPRK33 its three stage states, a 2N scheme the input of every stage
+  const double *A2, *B2, *C2;
+  int S2 = 0;
+  if (!ssp) rk2n_coefficients(ck2n, &A2, &B2, &C2, &S2);
+  const int P = ssp ? 3 : S2;
+  // checkpoints (nseg), the stage states of one segment (P K), step work (5), step-adjoint work (7)
   std::vector<void *> pool;
-  if ((st = adj_pool(c, (size_t)nseg + 3 * K + 12, vb, pool)) != IEQ_OK) return st;
-  std::vector<void *> ck(pool.begin(), pool.begin() + nseg), seg(pool.begin() + nseg, pool.begin() + nseg + 3 * K),
-      w(pool.begin() + nseg + 3 * K, pool.begin() + nseg + 3 * K + 5);
+  if ((st = adj_pool(c, (size_t)nseg + (size_t)P * K + 12, vb, pool)) != IEQ_OK) return st;
+  std::vector<void *> ck(pool.begin(), pool.begin() + nseg), seg(pool.begin() + nseg, pool.begin() + nseg + P * K),
+      w(pool.begin() + nseg + P * K, pool.begin() + nseg + P * K + 5);
   VjpWork vw;
-  vw.f.assign(pool.begin() + nseg + 3 * K + 5, pool.end());
+  vw.f.assign(pool.begin() + nseg + P * K + 5, pool.end());
   vw.d_time = c->adj_time + 2;
   void *cur = w[0], *b2 = w[1], *b3 = w[2], *cb = w[3], *uw = w[4];
   double *d_time = c->adj_time;
   std::vector<double> t0s(num_steps + 1, 0.0);
-  for (int n = 0; n < num_steps; ++n) t0s[n + 1] = t0s[n] + c->s.dt;   // calc_time_3_args
-  auto step = [&](void *state, double t0, void *keep1, void *keep2, void *keep3) -> ieq_status {
-    // one SSPRK33 step through the reference kernels, keeping the stage states
+  for (int n = 0; n < num_steps; ++n) t0s[n + 1] = t0s[n] + c->s.dt;   // calc_time_3_args / _2_args
+  // one step through the reference kernels; keep (optional) receives the P states of the step
+  auto step = [&](void *state, double t0, void *const *keep) -> ieq_status {
     double tt[2] = {t0, t0};
     cudaMemcpyAsync(d_time, tt, sizeof(tt), cudaMemcpyHostToDevice, c->stream);
-    if (keep1) cudaMemcpyAsync(keep1, state, vb, cudaMemcpyDeviceToDevice, c->stream);
     void *ua = c->s.variable_u ? uw : (void *)u;
-    void *args[7] = {state, b2, b3, cb, ua, (void *)rho, d_time};
-    const char *seq[] = {"calc_curlB_rho_1_3args", "calc_u_3_args", "SSPRK33_1", "SSPRK33_2a",
-                         "calc_curlB_rho_2_3args", "calc_u_3_args", "SSPRK33_2b", "SSPRK33_3a",
-                         "calc_curlB_rho_3_3args", "calc_u_3_args", "SSPRK33_3b"};
-    for (const char *k : seq) {
-      if (!c->s.hall && std::strncmp(k, "calc_curlB", 10) == 0) continue;
-      if (!c->s.variable_u && std::strncmp(k, "calc_u", 6) == 0) continue;
-      ieq_status s = adj_run_kernel(c, k, args, 7);
-      if (s != IEQ_OK) return s;
-      if (std::strcmp(k, "SSPRK33_1") == 0 && keep2) cudaMemcpyAsync(keep2, b2, vb, cudaMemcpyDeviceToDevice, c->stream);
-      if (std::strcmp(k, "SSPRK33_2b") == 0 && keep3) cudaMemcpyAsync(keep3, b3, vb, cudaMemcpyDeviceToDevice, c->stream);
+    if (ssp) {
+      if (keep) cudaMemcpyAsync(keep[0], state, vb, cudaMemcpyDeviceToDevice, c->stream);
+      void *args[7] = {state, b2, b3, cb, ua, (void *)rho, d_time};
+      const char *seq[] = {"calc_curlB_rho_1_3args", "calc_u_3_args", "SSPRK33_1", "SSPRK33_2a",
+                           "calc_curlB_rho_2_3args", "calc_u_3_args", "SSPRK33_2b", "SSPRK33_3a",
+                           "calc_curlB_rho_3_3args", "calc_u_3_args", "SSPRK33_3b"};
+      for (const char *k : seq) {
+        if (!c->s.hall && std::strncmp(k, "calc_curlB", 10) == 0) continue;
+        if (!c->s.variable_u && std::strncmp(k, "calc_u", 6) == 0) continue;
+        ieq_status s = adj_run_kernel(c, k, args, 7);
+        if (s != IEQ_OK) return s;
+        if (std::strcmp(k, "SSPRK33_1") == 0 && keep) cudaMemcpyAsync(keep[1], b2, vb, cudaMemcpyDeviceToDevice, c->stream);
+        if (std::strcmp(k, "SSPRK33_2b") == 0 && keep) cudaMemcpyAsync(keep[2], b3, vb, cudaMemcpyDeviceToDevice, c->stream);
+      }
+      return IEQ_OK;
     }
-    return IEQ_OK;
+    // 2N: for every stage the curl (Hall), the velocity (variable u), the "a" and the "b"
+    // kernel, then calc_time_2_args; b1 kept before every "a" kernel
+    void *args[6] = {state, b2, cb, ua, (void *)rho, d_time};
+    const std::string p = ck2n ? "CarpenterKennedy2N54_" : "ToulorgeDesmet2N84F_";
+    for (int s = 0; s < S2; ++s) {
+      if (keep) cudaMemcpyAsync(keep[s], state, vb, cudaMemcpyDeviceToDevice, c->stream);
+      ieq_status r;
+      if (c->s.hall && (r = adj_run_kernel(c, "calc_curlB_rho_1_2args", args, 6)) != IEQ_OK) return r;
+      if (c->s.variable_u && (r = adj_run_kernel(c, "calc_u_2_args", args, 6)) != IEQ_OK) return r;
+      if ((r = adj_run_kernel(c, (p + std::to_string(s + 1) + "a").c_str(), args, 6)) != IEQ_OK) return r;
+      if ((r = adj_run_kernel(c, (p + std::to_string(s + 1) + "b").c_str(), args, 6)) != IEQ_OK) return r;
+    }
+    return adj_run_kernel(c, "calc_time_2_args", args, 6);
   };
   // forward sweep with checkpoints
   cudaMemcpyAsync(cur, b0, vb, cudaMemcpyDeviceToDevice, c->stream);
   for (int n = 0; n < num_steps && st == IEQ_OK; ++n) {
     if (n % K == 0) cudaMemcpyAsync(ck[n / K], cur, vb, cudaMemcpyDeviceToDevice, c->stream);
-    st = step(cur, t0s[n], nullptr, nullptr, nullptr);
+    st = step(cur, t0s[n], nullptr);
   }
   // reverse sweep
   for (int s = nseg - 1; s >= 0 && st == IEQ_OK; --s) {
     const int n0 = s * K, n1 = std::min(num_steps, n0 + K);
     cudaMemcpyAsync(cur, ck[s], vb, cudaMemcpyDeviceToDevice, c->stream);
-    for (int n = n0; n < n1 && st == IEQ_OK; ++n)
-      st = step(cur, t0s[n], seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2]);
-    for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n)
-      st = ssprk33_step_vjp_ws(c, seg[3 * (n - n0)], seg[3 * (n - n0) + 1], seg[3 * (n - n0) + 2], t0s[n], lambda, u,
-                               rho, vw);
+    for (int n = n0; n < n1 && st == IEQ_OK; ++n) st = step(cur, t0s[n], &seg[(size_t)P * (n - n0)]);
+    for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n) {
+      void *const *x = &seg[(size_t)P * (n - n0)];
+      st = ssp ? ssprk33_step_vjp_ws(c, x[0], x[1], x[2], t0s[n], lambda, u, rho, vw)
+               : rk2n_step_vjp_ws(c, ck2n, x, t0s[n], lambda, u, rho, vw);
+    }
   }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "adjoint sweep");
   return st;

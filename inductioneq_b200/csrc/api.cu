@@ -734,6 +734,14 @@ ieq_status run_one_any(ieq_ctx *c, const char *name, const uint32_t *g, void *co
 #include "adjoint_args.inc"
 
 namespace ieq {
+// the coefficients of the 2N low-storage schemes (CarpenterKennedy2N54: ck = true;
+// ToulorgeDesmet2N84F) for adjoint.cu: A, B, C per stage and the stage count
+void rk2n_coefficients(bool ck, const double **A, const double **B, const double **C, int *stages) {
+  *A = ck ? kCK_A : kTD_A;
+  *B = ck ? kCK_B : kTD_B;
+  *C = ck ? kCK_C : kTD_C;
+  *stages = ck ? 5 : 8;
+}
 // pieces of a context that adjoint.cu needs to build its kernel arguments
 void adj_context(ieq_ctx *c, Mesh &m, const Tables<double> *&tab, double w[6], double inv_d[3], double two_inv_d[3],
                  double sat_s[3]) {

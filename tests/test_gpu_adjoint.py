@@ -5,7 +5,8 @@
 * the tangent against central differences of the forward operator;
 * the checkpointed SSPRK33 gradient of a final-time L2 misfit against central differences
   along seeded random directions (Richardson-extrapolated, relative 1e-6), driven through a torch.autograd.Function
-  (defined here, in the test harness only).
+  (defined here, in the test harness only);
+* the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F).
 """
 from __future__ import annotations
 
@@ -207,4 +208,74 @@ def test_repeated_sweeps_on_one_context_reuse_the_checkpoint_pool():
         fresh.close()
         assert np.array_equal(g, ref), p
     assert np.array_equal(got[0], got[3])
+    ctx.close()
+
+
+@pytest.mark.parametrize("integrator", ["CarpenterKennedy2N54", "ToulorgeDesmet2N84F"])
+def test_low_storage_step_adjoint_matches_central_differences(integrator):
+    # the checkpointed adjoint through the 2N low-storage schemes (stage by stage:
+    # mu2 += B_s mu1, mu1 += h F'^T mu2, mu2 = A_s mu2) against Richardson-extrapolated central
+    # differences of the forward time stepping, Hall periodic 16^3 with variable velocity
+    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16), integrator=integrator)
+    probe = maps_for(dict(c, dt=1.0)).context()
+    u = probe.vec()
+    probe.kernel("init_u", u)
+    umax = float(np.sqrt((probe.get_vec(u)[:, :3] ** 2).sum(1)).max())
+    probe.close()
+    dt = (2.0 / 16) * (HP / 16) / umax        # CFL 2/N (compute_error_hall_periodic.m:51)
+    ctx = maps_for(dict(c, dt=dt)).context()
+    nsteps, every = 9, 4
+    b = ctx.vec()
+    ctx.kernel("init_b", b)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    b0 = ctx.get_vec(b)
+    n = ctx.n
+    wmass = (HP / 16) ** 3
+
+    def forward(x):
+        bb, b2, cb, uu = ctx.vec(x), ctx.vec(), ctx.vec(), ctx.vec()
+        ctx.kernel("init_u", uu)
+        t = ctx.scalar(np.zeros(2), n=2)
+        ctx.time_steps(bb, b2, None, cb, uu, rho, t, nsteps)
+        return ctx.get_vec(bb)
+
+    rng = np.random.default_rng(11)
+    target = forward(b0) + 1e-3 * rng.standard_normal((ctx.n_pad, 4))
+    target[:, 3] = 0
+    target[n:] = 0
+
+    def loss(x):
+        d = forward(x)[:n, :3] - target[:n, :3]
+        return 0.5 * wmass * float(np.sum(d * d))
+
+    g0 = np.zeros_like(b0)
+    g0[:n, :3] = wmass * (forward(b0)[:n, :3] - target[:n, :3])
+    lam = ctx.vec(g0)
+    uu = ctx.vec()
+    ctx.kernel("init_u", uu)
+    ctx.adjoint_steps(ctx.vec(b0), lam, uu, rho, nsteps, every)
+    grad = ctx.get_vec(lam)
+    for k in range(4):
+        d = rng.standard_normal((ctx.n_pad, 4))
+        d[:, 3] = 0
+        d[n:] = 0
+        d /= np.sqrt(np.sum(d[:, :3] ** 2))
+        ad = float(np.sum(grad[:, :3] * d[:, :3]))
+
+        def cd(e):
+            return (loss(b0 + e * d) - loss(b0 - e * d)) / (2 * e)
+        rich = (4.0 * cd(5e-4) - cd(1e-3)) / 3.0
+        assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
+    ctx.close()
+
+
+def test_adjoint_of_an_unsupported_integrator_is_refused():
+    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16), integrator="KennedyCarpenterLewis2R54C")
+    ctx = maps_for(dict(c, dt=1e-3)).context()
+    b, u = ctx.vec(), ctx.vec()
+    lam = ctx.vec()
+    from inductioneq_b200.lib import IeqError
+    with pytest.raises(IeqError) as e:
+        ctx.adjoint_steps(b, lam, u, ctx.scalar(np.ones(ctx.n_pad)), 2, 1)
+    assert e.value.name == "IEQ_ERR_SETTINGS"
     ctx.close()

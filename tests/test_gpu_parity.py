@@ -684,3 +684,32 @@ def test_cg_host_loop_equals_graph_loop():
         ctx.close()
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
     np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+FLUX_FORMS = [(ui, so, uj) for ui in ("CENTRAL", "SPLIT", "PRODUCT") for so in ("ZERO", "CENTRAL", "SPLIT")
+              for uj in ("CENTRAL", "SPLIT", "PRODUCT")]
+
+
+@pytest.mark.parametrize("uibj, source, ujbi", FLUX_FORMS)
+def test_every_flux_form_combination_matches_oracle(uibj, source, ujbi):
+    # the 27 combinations of USE_UIBJ_* / USE_SOURCE_* / USE_UJBI_* (induction_Eq_volume.cl:
+    # 13-212) with convection (rigid rotation on a box, inflow SAT), one SSPRK33 step through
+    # the fused path and through the reference kernel list, against the oracle
+    c = dict(order=4, testcase="rotation_gaussian", nodes=(12, 13, 11), lo=-1.0, hi=1.0, integrator="SSPRK33",
+             dt=0.01, uibj=uibj, source=source, ujbi=ujbi)
+    o = oracle_for(c)
+    b, u = o.vec(), o.vec()
+    o.run("init_b", o.cfg.nodes, b)
+    o.run("init_u", o.cfg.nodes, u)
+    b[:, :3] += 1e-2 * np.random.default_rng(NOISE_SEED).standard_normal((o.N, 3))
+    host = [b.copy(), o.vec(), o.vec(), o.vec(), u, o.scalar(fill=1.0), np.zeros(2)]
+    time_loop(o, "SSPRK33", False, False, 1, host[0], host[1], host[2], host[3], host[4], host[5], host[6])
+    for kernel in ("AUTO", "LIST"):
+        ctx = maps_for(dict(c, stage_kernel=kernel)).context()
+        dev = [ctx.vec(b), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(u), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.time_steps(*dev, 1)
+        for i in (0, 1, 2):
+            e = rel_err(ctx.get_vec(dev[i])[: o.N], host[i])
+            assert e <= 1e-12, (kernel, i, e)
+        ctx.close()
