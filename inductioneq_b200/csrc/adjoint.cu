@@ -1,11 +1,15 @@
-// adjoint.cu -- discrete adjoint of the semi-discretisation and of SSPRK33.
+// adjoint.cu -- discrete adjoint of the semi-discretisation and of the SSPRK33 and 2N
+// low-storage steps.
 //
 // F(b) is the time derivative DB of kernel/kernel_time_integrator.cl:9-31 (volume terms,
 // Hall term with J = curl(b)/rho, artificial dissipation, inflow SAT) at fixed u and rho.
-// Three operators are provided, all FP64:
+// The operators, all FP64:
 //   jvp:  F'(b0) v    (tangent linear; used by the transpose tests)
 //   vjp:  F'(b0)^T w  (the adjoint of the spatial operator)
-//   SSPRK33 step adjoint: lambda_n = (d b_{n+1} / d b_n)^T lambda_{n+1} from the stage states
+//   step adjoints: lambda_n = (d b_{n+1} / d b_n)^T lambda_{n+1} from the stage states
+//   (SSPRK33; CarpenterKennedy2N54 and ToulorgeDesmet2N84F from the input of every stage),
+//   and the checkpointed sweep over many steps, whose forward passes run the fused stage
+//   kernels of the time stepping with the stage states written out per stage
 // The transposes are written out per term (see the notes at k_vjp_pass1); D^T is applied as
 // a gather over the neighbours j = k + p with the coefficient of row(j) at offset -p.
 // The Hall outflow SAT (a switch on the sign of 0.5u - J) has no adjoint here: Hall runs
@@ -33,6 +37,11 @@ struct AdjArgs {
   const double *rho;
   R4<double> *out;
   R4<double> *gJr;       // vjp pass 1 -> pass 2: (Hall adjoint source for J) / rho
+  // epilogue of the vjp's last kernel (dst != nullptr): dst = eal ex + ebe ey + ega z instead
+  // of out = z (ex, ey may be null; dst may be ex or ey, never v)
+  R4<double> *dst;
+  const R4<double> *ex, *ey;
+  double eal, ebe, ega;
 };
 
 __device__ __forceinline__ V3<double> ld(const R4<double> *p, long long j) { return ld3(p + j); }
@@ -190,13 +199,84 @@ __global__ void k_jvp(const AdjArgs a) {
   st3(a.out + k, out);
 }
 
+// Nodes on which every derivative row involved is the interior row of half-width RI: every
+// node of a periodic grid, and on a box the nodes at least nb + (SW-1)/2 from every face
+// (no boundary row of a neighbour reaches them).  There D^T at the node gathers d[-p] f(k+p)
+// and D gathers d[p] f(k+p), d the interior row; RI = 0 when the interior row has entries
+// beyond the order's half-width (then every node takes the generic row lookups).
+template <int RI>
+__device__ __forceinline__ bool fast_node(const AdjArgs &a, const Node &nd) {
+  if (RI == 0) return false;
+  if (a.periodic) return true;
+  const int lo = a.nb + (a.sw - 1) / 2;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax)
+    if (nd.i[ax] < lo || nd.i[ax] > nd.n[ax] - 1 - lo) return false;
+  return true;
+}
+
+// neighbour k + o along ax on the fast path (periodic wrap; interior nodes need none)
+__device__ __forceinline__ long long fnbr(const AdjArgs &a, const Node &nd, int ax, int o) {
+  int t = nd.i[ax] + o;
+  if (a.periodic) {
+    t += (t < 0) ? nd.n[ax] : 0;
+    t -= (t >= nd.n[ax]) ? nd.n[ax] : 0;
+  }
+  return nd.idx + (long long)(t - nd.i[ax]) * nd.st[ax];
+}
+
+// the interior row d[o + RI] = D[nb][(SW-1)/2 + o]
+template <int RI>
+__device__ __forceinline__ void interior_row(const AdjArgs &a, double (&d)[2 * RI + 1]) {
+  const int c0 = (a.sw - 1) / 2;
+#pragma unroll
+  for (int o = -RI; o <= RI; ++o) d[o + RI] = a.tab->D[a.nb][c0 + o];
+}
+
+// the terms of one axis of F'(b0)^T w at the node from q = D_ax^T w, Du = D_ax u,
+// S3 = D_ax^T (u . w), S5 = D_ax^T (u_ax w)
+__device__ __forceinline__ void pass1_axis(const AdjArgs &a, int ax, V3<double> q, V3<double> Du, double S3,
+                                           V3<double> S5, V3<double> wm, V3<double> um, V3<double> b0m,
+                                           V3<double> J0m, V3<double> &z, V3<double> &gJ) {
+  if (a.conv) {
+    const double ua = comp(um, ax), Dua = comp(Du, ax);
+    addc(z, ax, a.two_inv_d[ax] * (a.w[0] * dot3(um, q) + a.w[1] * dot3(Du, wm) + a.w[2] * S3));
+    for (int i = 0; i < 3; ++i)
+      addc(z, i, -a.two_inv_d[ax] * (a.w[3] * ua * comp(q, i) + a.w[4] * comp(S5, i) + a.w[5] * Dua * comp(wm, i)));
+  }
+  if (a.hall) {
+    const V3<double> Q = {q.x * a.inv_d[ax], q.y * a.inv_d[ax], q.z * a.inv_d[ax]};
+    const double J0a = comp(J0m, ax), b0a = comp(b0m, ax);
+    z = axpy3(J0a, Q, z);
+    addc(z, ax, -dot3(J0m, Q));
+    addc(gJ, ax, dot3(b0m, Q));
+    gJ = axpy3(-b0a, Q, gJ);
+  }
+}
+
+// the vjp's result at node k: out = z, or the epilogue dst = eal ex + ebe ey + ega z (the
+// operation order of k_lincomb)
+__device__ __forceinline__ void vjp_store(const AdjArgs &a, long long k, V3<double> z) {
+  if (!a.dst) {
+    st3(a.out + k, z);
+    return;
+  }
+  V3<double> r = {0, 0, 0};
+  if (a.ex) r = axpy3(a.eal, ld3_plain(a.ex + k), r);
+  if (a.ey) r = axpy3(a.ebe, ld3_plain(a.ey + k), r);
+  r = axpy3(a.ega, z, r);
+  st3(a.dst + k, r);
+}
+
 // F'(b0)^T w, pass 1.  With q_a = D_a^T w (per component), the forward terms transpose to
 //   D_a[u_i b_a]      -> z_a += sum_i u_i q_a,i          b_a D_a[u_i] -> z_a += D_a[u] . w
 //   u_i D_a[b_a]      -> z_a += D_a^T[u . w]             D_a[u_a b_i] -> z_i += u_a q_a,i
 //   u_a D_a[b_i]      -> z_i += D_a^T[u_a w_i]           b_i D_a[u_a] -> z_i += D_a[u_a] w_i
 // (times the flux-form weights and 2/d_a); the Hall term with Q_a = q_a / d_a gives
 //   z_i += J0_a Q_a,i,  z_a -= J0 . Q_a,  and the source for dJ: gJ = sum_a (b0.Q_a) e_a - b0_a Q_a,
-// whose curl transpose (pass 2) adds C^T (gJ / rho).
+// whose curl transpose (pass 2) adds C^T (gJ / rho).  On fast nodes the four gathers of an
+// axis share one pass over the neighbours (u and w loaded once per neighbour).
+template <int RI>
 __global__ void k_vjp_pass1(const AdjArgs a) {
   Node nd;
   if (!make_node(a, nd)) return;
@@ -204,62 +284,116 @@ __global__ void k_vjp_pass1(const AdjArgs a) {
   const V3<double> wm = ld(a.v, k), um = a.conv ? ld(a.u, k) : V3<double>{0, 0, 0};
   V3<double> z = {0, 0, 0}, gJ = {0, 0, 0};
   V3<double> b0m = {0, 0, 0}, J0m = {0, 0, 0};
-  if (a.hall) {
-    b0m = ld(a.b0, k);
-    J0m = ld(a.J0, k);
-  }
-  for (int ax = 0; ax < 3; ++ax) {
-    const V3<double> q = dtr(a, nd, ax, [&](long long j) { return ld(a.v, j); });
-    if (a.conv) {
-      const V3<double> Du = dfwd(a, nd, ax, [&](long long j) { return ld(a.u, j); });
-      const V3<double> S3 = dtr(a, nd, ax, [&](long long j) {
-        const double s = dot3(ld(a.u, j), ld(a.v, j));
-        return V3<double>{s, 0, 0};
-      });
-      const V3<double> S5 = dtr(a, nd, ax, [&](long long j) {
-        const double ua = comp(ld(a.u, j), ax);
-        const V3<double> ww = ld(a.v, j);
-        return V3<double>{ua * ww.x, ua * ww.y, ua * ww.z};
-      });
-      const double ua = comp(um, ax), Dua = comp(Du, ax);
-      addc(z, ax, a.two_inv_d[ax] * (a.w[0] * dot3(um, q) + a.w[1] * dot3(Du, wm) + a.w[2] * S3.x));
-      for (int i = 0; i < 3; ++i)
-        addc(z, i, -a.two_inv_d[ax] * (a.w[3] * ua * comp(q, i) + a.w[4] * comp(S5, i) + a.w[5] * Dua * comp(wm, i)));
-    }
+  if (a.hall) b0m = ld(a.b0, k);
+  if (fast_node<RI>(a, nd)) {
+    double d[2 * RI + 1];
+    interior_row<RI>(a, d);
     if (a.hall) {
-      const V3<double> Q = {q.x * a.inv_d[ax], q.y * a.inv_d[ax], q.z * a.inv_d[ax]};
-      const double J0a = comp(J0m, ax), b0a = comp(b0m, ax);
-      z = axpy3(J0a, Q, z);
-      addc(z, ax, -dot3(J0m, Q));
-      addc(gJ, ax, dot3(b0m, Q));
-      gJ = axpy3(-b0a, Q, gJ);
+      // J0 = curl(b0) / rho at the node (as k_curl_rho: interior rows times 1/d, then 1/rho)
+      double g[3][3];
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const int c1 = (ax + 1) % 3, c2 = (ax + 2) % 3;
+        double v1 = 0, v2 = 0;
+#pragma unroll
+        for (int o = -RI; o <= RI; ++o) {
+          if (o == 0) continue;
+          const V3<double> bj = ld(a.b0, fnbr(a, nd, ax, o));
+          v1 += d[RI + o] * comp(bj, c1);
+          v2 += d[RI + o] * comp(bj, c2);
+        }
+        g[ax][c1] = v1 * a.inv_d[ax];
+        g[ax][c2] = v2 * a.inv_d[ax];
+      }
+      const double r = 1.0 / a.rho[k];
+      J0m = {(g[1][2] - g[2][1]) * r, (g[2][0] - g[0][2]) * r, (g[0][1] - g[1][0]) * r};
     }
-    if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      V3<double> q = {0, 0, 0}, Du = {0, 0, 0}, S5 = {0, 0, 0};
+      double S3 = 0.0;
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) {
+        const double ct = d[RI - o], cf = d[RI + o];
+        V3<double> vj = wm, uj = um;
+        if (o != 0) {
+          const long long j = fnbr(a, nd, ax, o);
+          vj = ld(a.v, j);
+          if (a.conv) uj = ld(a.u, j);
+        }
+        q = axpy3(ct, vj, q);
+        if (a.conv) {
+          Du = axpy3(cf, uj, Du);
+          S3 += ct * dot3(uj, vj);
+          const double uja = comp(uj, ax);
+          S5 = axpy3(ct, V3<double>{uja * vj.x, uja * vj.y, uja * vj.z}, S5);
+        }
+      }
+      pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
+      if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+    }
+  } else {
+    if (a.hall) J0m = ld(a.J0, k);
+    for (int ax = 0; ax < 3; ++ax) {
+      const V3<double> q = dtr(a, nd, ax, [&](long long j) { return ld(a.v, j); });
+      V3<double> Du = {0, 0, 0}, S5 = {0, 0, 0};
+      double S3 = 0.0;
+      if (a.conv) {
+        Du = dfwd(a, nd, ax, [&](long long j) { return ld(a.u, j); });
+        S3 = dtr(a, nd, ax, [&](long long j) {
+          const double s = dot3(ld(a.u, j), ld(a.v, j));
+          return V3<double>{s, 0, 0};
+        }).x;
+        S5 = dtr(a, nd, ax, [&](long long j) {
+          const double ua = comp(ld(a.u, j), ax);
+          const V3<double> ww = ld(a.v, j);
+          return V3<double>{ua * ww.x, ua * ww.y, ua * ww.z};
+        });
+      }
+      pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
+      if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+    }
   }
   z = axpy3(sat_diag(a, nd, um), wm, z);
-  st3(a.out + k, z);
   if (a.hall) {
+    st3(a.out + k, z);
     const double r = 1.0 / a.rho[k];
     st3(a.gJr + k, V3<double>{gJ.x * r, gJ.y * r, gJ.z * r});
+  } else {
+    vjp_store(a, k, z);
   }
 }
 
 // pass 2: z += C^T g with C the SBP curl (rows / d), g = gJ / rho
+template <int RI>
 __global__ void k_vjp_pass2(const AdjArgs a) {
   Node nd;
   if (!make_node(a, nd)) return;
   const long long k = nd.idx;
   V3<double> g[3];
-  for (int ax = 0; ax < 3; ++ax) {
-    const V3<double> t = dtr(a, nd, ax, [&](long long j) { return ld(a.gJr, j); });
-    g[ax] = {t.x * a.inv_d[ax], t.y * a.inv_d[ax], t.z * a.inv_d[ax]};   // (D_ax^T g_c) / d_ax
+  if (fast_node<RI>(a, nd)) {
+    double d[2 * RI + 1];
+    interior_row<RI>(a, d);
+    const V3<double> gm = ld(a.gJr, k);
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      V3<double> t = {0, 0, 0};
+#pragma unroll
+      for (int o = -RI; o <= RI; ++o) t = axpy3(d[RI - o], o == 0 ? gm : ld(a.gJr, fnbr(a, nd, ax, o)), t);
+      g[ax] = {t.x * a.inv_d[ax], t.y * a.inv_d[ax], t.z * a.inv_d[ax]};
+    }
+  } else {
+    for (int ax = 0; ax < 3; ++ax) {
+      const V3<double> t = dtr(a, nd, ax, [&](long long j) { return ld(a.gJr, j); });
+      g[ax] = {t.x * a.inv_d[ax], t.y * a.inv_d[ax], t.z * a.inv_d[ax]};   // (D_ax^T g_c) / d_ax
+    }
   }
   // (C^T g)_x = Dz^T g_y - Dy^T g_z, (C^T g)_y = Dx^T g_z - Dz^T g_x, (C^T g)_z = Dy^T g_x - Dx^T g_y
   V3<double> z = ld3_plain(a.out + k);
   z.x += g[2].y - g[1].z;
   z.y += g[0].z - g[2].x;
   z.z += g[1].x - g[0].y;
-  st3(a.out + k, z);
+  vjp_store(a, k, z);
 }
 
 // out = alpha*x + beta*y (+ gamma*z) over the nodes (x, y, z may be the same array as out)
@@ -285,6 +419,10 @@ void adj_curl(ieq_ctx *c, const void *b, const void *rho, void *out);
 void rk2n_coefficients(bool ck, const double **A, const double **B, const double **C, int *stages);
 void adj_context(ieq_ctx *c, Mesh &m, const Tables<double> *&tab, double w[6], double inv_d[3], double two_inv_d[3],
                  double sat_s[3]);
+// from api_fused.inc
+ieq_status adj_fused_steps(ieq_ctx *c, int conv, void *b, void *b2, void *b3, void *cb, void *u, const void *rho,
+                           void *time, int nsteps, void *const *keep, int P);
+ieq_status adj_read_conv(ieq_ctx *c, const void *u, int &conv);
 
 AdjArgs adj_args(ieq_ctx *c) {
   AdjArgs a;
@@ -318,6 +456,15 @@ ieq_status check_adjoint_settings(ieq_ctx *c) {
   return IEQ_OK;
 }
 
+// half-width of the vjp kernels' interior fast path: order/2 when the interior derivative row
+// has no entries beyond it, else 0 (generic row lookups on every node)
+int fast_ri(const ieq_ctx *c) {
+  const int ri = c->op.order / 2, c0 = (c->op.sw - 1) / 2;
+  for (int k = 0; k < c->op.sw; ++k)
+    if (std::abs(k - c0) > ri && c->op.D.at(c->op.nb, k) != 0.0) return 0;
+  return ri;
+}
+
 dim3 ablock() { return dim3(32, 4, 2); }
 dim3 agrid(const ieq_ctx *c) {
   return dim3((c->s.nodes[0] + 31) / 32, (c->s.nodes[1] + 3) / 4, (c->s.nodes[2] + 1) / 2);
@@ -343,21 +490,46 @@ void free_all(std::vector<void *> &bufs) {
 }
 
 // out = F'(b)^T w (u at the stage time, rho); J0, gJr: work fields
+// optional epilogue of vjp: dst = al x + be y + ga F'(b)^T w (x, y may be null)
+struct Epi {
+  void *dst = nullptr;
+  const void *x = nullptr, *y = nullptr;
+  double al = 0, be = 0, ga = 0;
+};
+
 ieq_status vjp(ieq_ctx *c, const void *b, const void *w, const void *u, const void *rho, void *out, void *J0,
-               void *gJr) {
+               void *gJr, const Epi &epi = Epi()) {
   AdjArgs a = adj_args(c);
+  a.dst = (R4<double> *)epi.dst;
+  a.ex = (const R4<double> *)epi.x;
+  a.ey = (const R4<double> *)epi.y;
+  a.eal = epi.al;
+  a.ebe = epi.be;
+  a.ega = epi.ga;
   a.b0 = (const R4<double> *)b;
   a.u = (const R4<double> *)u;
   a.v = (const R4<double> *)w;
   a.rho = (const double *)rho;
   a.out = (R4<double> *)out;
   a.gJr = (R4<double> *)gJr;
-  if (c->s.hall) {
+  if (c->s.hall && fast_ri(c) == 0) {   // else pass 1 forms J0 at the node itself
     adj_curl(c, b, rho, J0);
     a.J0 = (const R4<double> *)J0;
   }
-  k_vjp_pass1<<<agrid(c), ablock(), 0, c->stream>>>(a);
-  if (c->s.hall) k_vjp_pass2<<<agrid(c), ablock(), 0, c->stream>>>(a);
+  switch (fast_ri(c)) {
+    case 1: k_vjp_pass1<1><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+    case 2: k_vjp_pass1<2><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+    case 3: k_vjp_pass1<3><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+    default: k_vjp_pass1<0><<<agrid(c), ablock(), 0, c->stream>>>(a);
+  }
+  if (c->s.hall) {
+    switch (fast_ri(c)) {
+      case 1: k_vjp_pass2<1><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+      case 2: k_vjp_pass2<2><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+      case 3: k_vjp_pass2<3><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
+      default: k_vjp_pass2<0><<<agrid(c), ablock(), 0, c->stream>>>(a);
+    }
+  }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? IEQ_OK : afail(c, IEQ_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -408,18 +580,19 @@ ieq_status ssprk33_step_vjp_ws(ieq_ctx *c, const void *s1, const void *s2, const
   const double h = c->s.dt;
   const double t2 = t0 + h, t3 = t0 + 0.5 * h;   // SSPRK33_2a / _3a
   ieq_status st;
+  // the combinations with F'^T are the vjp's epilogue
+  Epi e;
   // stage 3: lambda3 = 2/3 (lambda + h F'(s3)^T lambda); lambda1 = 1/3 lambda
-  if ((st = vjp(c, s3, lambda, stage_u(c, u, uw, d_time, t3), rho, z, J0, gJr)) != IEQ_OK) return st;
-  lincomb(c, l3, 2.0 / 3.0, lambda, 2.0 / 3.0 * h, z);
+  e.dst = l3; e.x = lambda; e.al = 2.0 / 3.0; e.ga = 2.0 / 3.0 * h;
+  if ((st = vjp(c, s3, lambda, stage_u(c, u, uw, d_time, t3), rho, z, J0, gJr, e)) != IEQ_OK) return st;
   lincomb(c, l1, 1.0 / 3.0, lambda, 0.0, nullptr);
   // stage 2: lambda2 = 1/4 (lambda3 + h F'(s2)^T lambda3); lambda1 += 3/4 lambda3
-  if ((st = vjp(c, s2, l3, stage_u(c, u, uw, d_time, t2), rho, z, J0, gJr)) != IEQ_OK) return st;
-  lincomb(c, l2, 0.25, l3, 0.25 * h, z);
+  e.dst = l2; e.x = l3; e.al = 0.25; e.ga = 0.25 * h;
+  if ((st = vjp(c, s2, l3, stage_u(c, u, uw, d_time, t2), rho, z, J0, gJr, e)) != IEQ_OK) return st;
   lincomb(c, l1, 1.0, l1, 0.75, l3);
   // stage 1: lambda1 += lambda2 + h F'(s1)^T lambda2
-  if ((st = vjp(c, s1, l2, stage_u(c, u, uw, d_time, t0), rho, z, J0, gJr)) != IEQ_OK) return st;
-  lincomb(c, lambda, 1.0, l1, 1.0, l2, h, z);
-  return IEQ_OK;
+  e.dst = lambda; e.x = l1; e.y = l2; e.al = 1.0; e.be = 1.0; e.ga = h;
+  return vjp(c, s1, l2, stage_u(c, u, uw, d_time, t0), rho, z, J0, gJr, e);
 }
 
 // lambda <- (d step / d b_n)^T lambda for one step of a 2N low-storage scheme
@@ -429,7 +602,8 @@ ieq_status ssprk33_step_vjp_ws(ieq_ctx *c, const void *s1, const void *s2, const
 // reversed with mu1 = lambda (b1 after the step) and mu2 = 0 (the next step's first stage has
 // A_0 = 0, so b2 after a step does not reach the next):
 //   mu2 += B_s mu1;  mu1 += h F'(x[s], t_s)^T mu2;  mu2 = A_s mu2      (s = S-1 .. 0)
-// w.f[3] holds mu2; no allocation, no synchronisation
+// (the scaling by A_s and the next stage's B_{s-1} mu1 in one pass; mu1 += h F'^T mu2 as the
+// vjp's epilogue).  w.f[3] holds mu2; no allocation, no synchronisation
 ieq_status rk2n_step_vjp_ws(ieq_ctx *c, bool ck, void *const *x, double t0, void *lambda, const void *u,
                             const void *rho, const VjpWork &w) {
   void *J0 = w.f[0], *gJr = w.f[1], *z = w.f[2], *mu2 = w.f[3], *uw = w.f[6];
@@ -437,14 +611,14 @@ ieq_status rk2n_step_vjp_ws(ieq_ctx *c, bool ck, void *const *x, double t0, void
   int S;
   rk2n_coefficients(ck, &A, &B, &C, &S);
   const double h = c->s.dt;
-  cudaMemsetAsync(mu2, 0, c->n_pad * sizeof(R4<double>), c->stream);
   ieq_status st;
+  Epi e;
+  e.dst = lambda; e.x = lambda; e.al = 1.0; e.ga = h;
   for (int s = S - 1; s >= 0; --s) {
     const double ts = s == 0 ? t0 : t0 + C[s - 1] * h;
-    lincomb(c, mu2, 1.0, mu2, B[s], lambda);
-    if ((st = vjp(c, x[s], mu2, stage_u(c, u, uw, w.d_time, ts), rho, z, J0, gJr)) != IEQ_OK) return st;
-    lincomb(c, lambda, 1.0, lambda, h, z);
-    lincomb(c, mu2, A[s], mu2, 0.0, nullptr);
+    if (s == S - 1) lincomb(c, mu2, B[s], lambda, 0.0, nullptr);   // mu2 = 0 + B_s mu1
+    else lincomb(c, mu2, A[s + 1], mu2, B[s], lambda);             // A_{s+1} mu2 + B_s mu1
+    if ((st = vjp(c, x[s], mu2, stage_u(c, u, uw, w.d_time, ts), rho, z, J0, gJr, e)) != IEQ_OK) return st;
   }
   return IEQ_OK;
 }
@@ -564,17 +738,24 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   double *d_time = c->adj_time;
   std::vector<double> t0s(num_steps + 1, 0.0);
   for (int n = 0; n < num_steps; ++n) t0s[n + 1] = t0s[n] + c->s.dt;   // calc_time_3_args / _2_args
-  // one step through the reference kernels; keep (optional) receives the P states of the step
-  auto step = [&](void *state, double t0, void *const *keep) -> ieq_status {
-    double tt[2] = {t0, t0};
+  // the forward passes run the fused stage kernels (ieq_time_steps' path) unless the settings
+  // ask for the reference kernel lists (IEQ_STAGE_KERNEL=LIST)
+  const bool fused = c->s.stage_kernel != 4;
+  int conv = 1;
+  if (fused && (st = adj_read_conv(c, u, conv)) != IEQ_OK) return st;
+  void *ua = c->s.variable_u ? uw : (void *)u;   // u is rewritten only when it varies in time
+  auto set_time = [&](double t0) {
+    const double tt[2] = {t0, t0};
     cudaMemcpyAsync(d_time, tt, sizeof(tt), cudaMemcpyHostToDevice, c->stream);
-    void *ua = c->s.variable_u ? uw : (void *)u;
+  };
+  // one step through the reference kernels; keep (optional) receives the P states of the step
+  auto step = [&](void *state, void *const *keep) -> ieq_status {
     if (ssp) {
       if (keep) cudaMemcpyAsync(keep[0], state, vb, cudaMemcpyDeviceToDevice, c->stream);
       void *args[7] = {state, b2, b3, cb, ua, (void *)rho, d_time};
       const char *seq[] = {"calc_curlB_rho_1_3args", "calc_u_3_args", "SSPRK33_1", "SSPRK33_2a",
                            "calc_curlB_rho_2_3args", "calc_u_3_args", "SSPRK33_2b", "SSPRK33_3a",
-                           "calc_curlB_rho_3_3args", "calc_u_3_args", "SSPRK33_3b"};
+                           "calc_curlB_rho_3_3args", "calc_u_3_args", "SSPRK33_3b", "calc_time_3_args"};
       for (const char *k : seq) {
         if (!c->s.hall && std::strncmp(k, "calc_curlB", 10) == 0) continue;
         if (!c->s.variable_u && std::strncmp(k, "calc_u", 6) == 0) continue;
@@ -599,17 +780,27 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
     }
     return adj_run_kernel(c, "calc_time_2_args", args, 6);
   };
-  // forward sweep with checkpoints
+  // nsteps steps of `state` from time t0, the stage states of step k into keep[P k ..] if given
+  auto advance = [&](void *state, double t0, int nsteps, void *const *keep) -> ieq_status {
+    set_time(t0);
+    if (fused) return adj_fused_steps(c, conv, state, b2, b3, cb, ua, rho, d_time, nsteps, keep, P);
+    ieq_status r = IEQ_OK;
+    for (int k = 0; k < nsteps && r == IEQ_OK; ++k) r = step(state, keep ? keep + (size_t)P * k : nullptr);
+    return r;
+  };
+  // forward sweep: the checkpoints at the start of every segment (the last segment's steps are
+  // run by the reverse sweep only)
   cudaMemcpyAsync(cur, b0, vb, cudaMemcpyDeviceToDevice, c->stream);
-  for (int n = 0; n < num_steps && st == IEQ_OK; ++n) {
-    if (n % K == 0) cudaMemcpyAsync(ck[n / K], cur, vb, cudaMemcpyDeviceToDevice, c->stream);
-    st = step(cur, t0s[n], nullptr);
+  for (int s = 0; s < nseg && st == IEQ_OK; ++s) {
+    cudaMemcpyAsync(ck[s], cur, vb, cudaMemcpyDeviceToDevice, c->stream);
+    if (s + 1 < nseg) st = advance(cur, t0s[(size_t)s * K], K, nullptr);
   }
-  // reverse sweep
+  // reverse sweep: recompute a segment from its checkpoint keeping the stage states, then
+  // apply the step adjoints backwards
   for (int s = nseg - 1; s >= 0 && st == IEQ_OK; --s) {
     const int n0 = s * K, n1 = std::min(num_steps, n0 + K);
     cudaMemcpyAsync(cur, ck[s], vb, cudaMemcpyDeviceToDevice, c->stream);
-    for (int n = n0; n < n1 && st == IEQ_OK; ++n) st = step(cur, t0s[n], &seg[(size_t)P * (n - n0)]);
+    st = advance(cur, t0s[n0], n1 - n0, seg.data());
     for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n) {
       void *const *x = &seg[(size_t)P * (n - n0)];
       st = ssp ? ssprk33_step_vjp_ws(c, x[0], x[1], x[2], t0s[n], lambda, u, rho, vw)

@@ -279,3 +279,33 @@ def test_adjoint_of_an_unsupported_integrator_is_refused():
         ctx.adjoint_steps(b, lam, u, ctx.scalar(np.ones(ctx.n_pad)), 2, 1)
     assert e.value.name == "IEQ_ERR_SETTINGS"
     ctx.close()
+
+
+@pytest.mark.parametrize("name, integrator", [("hallper_4c", "SSPRK33"), ("rot_6c_sat", "SSPRK33"),
+                                              ("rot3d_4e_split_hod", "CarpenterKennedy2N54"),
+                                              ("hallper_6c_hod", "ToulorgeDesmet2N84F")])
+def test_sweep_on_fused_forward_equals_sweep_on_reference_kernel_lists(name, integrator):
+    # the sweep's forward passes run the fused stage kernels (their stage states written out
+    # per stage); with IEQ_STAGE_KERNEL=LIST they run the reference kernel lists.  Both
+    # linearise about the same trajectory up to rounding: the gradients agree to 1e-11 of
+    # their scale.  10 steps with checkpoints every 4: a short last segment.
+    c = dict(CASES[name], integrator=integrator)
+    probe = maps_for(dict(c, dt=1.0)).context()
+    u = probe.vec()
+    probe.kernel("init_u", u)
+    umax = max(float(np.sqrt((probe.get_vec(u)[:, :3] ** 2).sum(1)).max()), 1.0)
+    probe.close()
+    lo, hi = c["lo"], c["hi"]
+    dt = 0.2 * (hi - lo) / max(c["nodes"]) / umax
+    out = []
+    for kernel in ("AUTO", "LIST"):
+        ctx = maps_for(dict(c, dt=dt, stage_kernel=kernel)).context()
+        b, u = ctx.vec(), ctx.vec()
+        ctx.kernel("init_b", b)
+        ctx.kernel("init_u", u)
+        lam = ctx.vec(_rand(ctx, 5))
+        ctx.adjoint_steps(b, lam, u, ctx.scalar(np.ones(ctx.n_pad)), 10, 4)
+        out.append(ctx.get_vec(lam)[:, :3])
+        ctx.close()
+    scale = np.abs(out[1]).max()
+    assert np.abs(out[0] - out[1]).max() <= 1e-11 * scale
