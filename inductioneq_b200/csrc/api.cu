@@ -23,7 +23,7 @@ using namespace ieq;
 namespace {
 
 constexpr int kReduceBlocks = 592;   // 4 x 148 SMs; fixed so that sums are reproducible
-constexpr int kMaxPartials = 65536;  // CG fused-dot partials (one per stencil block)
+constexpr int kMaxPartials = 65536;  // least size of the block-partial buffers (CG passes, diagnostics)
 // grids from which IEQ_STAGE_KERNEL=AUTO runs the one-pass Hall stage (stage_z.cuh).
 // Measured on B200 (whistler, 6th order + HOD, FP64): 1.73 ms per stage at 256^3 against
 // 0.78 ms for the curl + stage pair (0.22 / 0.69 ms at 128^3): its shared-memory E ring
@@ -826,8 +826,14 @@ ieq_status ieq_create(ieq_ctx **out, const char *settings, const char *const *pa
   };
   cuda(cudaSetDevice(device), "cudaSetDevice");
   if (st == IEQ_OK) cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-  if (st == IEQ_OK) cuda(cudaMalloc(&c->d_partials, kMaxPartials * sizeof(double)), "cudaMalloc");
-  if (st == IEQ_OK) cuda(cudaMalloc(&c->d_partials2, kMaxPartials * sizeof(double)), "cudaMalloc");
+  // one partial per block of the finest grid the one-pass reductions launch (128 threads over
+  // 32 x 2 x 2 nodes), three per block for the diagnostics
+  {
+    const long long bx = (c->s.nodes[0] + 31) / 32, by = (c->s.nodes[1] + 1) / 2, bz = (c->s.nodes[2] + 1) / 2;
+    c->partials_cap = std::max<long long>(kMaxPartials, 3 * bx * by * bz);
+  }
+  if (st == IEQ_OK) cuda(cudaMalloc(&c->d_partials, c->partials_cap * sizeof(double)), "cudaMalloc");
+  if (st == IEQ_OK) cuda(cudaMalloc(&c->d_partials2, c->partials_cap * sizeof(double)), "cudaMalloc");
   if (st == IEQ_OK) cuda(cudaMalloc(&c->d_total, 64 * sizeof(double)), "cudaMalloc");
   if (st == IEQ_OK) cuda(cudaMalloc(&c->d_counter, 64 * sizeof(unsigned)), "cudaMalloc");
   if (st == IEQ_OK) cuda(cudaMemset(c->d_counter, 0, 64 * sizeof(unsigned)), "cudaMemset");

@@ -114,6 +114,7 @@ struct ieq_ctx {
   // scratch
   double *d_partials = nullptr;    // reduction partials
   double *d_partials2 = nullptr;
+  long long partials_cap = 0;      // entries of d_partials and d_partials2
   double *d_total = nullptr;       // reduction totals
   unsigned *d_counter = nullptr;   // last-block tickets
   int *d_flag = nullptr;

@@ -684,8 +684,9 @@ __global__ void __launch_bounds__(kCgTX * kCgTY) k_cg_pass_a_z(const LapArgs<dou
 }
 
 // Pass B (clean_div.m:57-66): phi += alpha*u (calc_xpay), r -= alpha*lap, rr = <r, r> (last
-// block), then the loop condition of clean_div.m:47, written to the graph loop's condition
-template <typename S>
+// block), then the loop condition of clean_div.m:47, written to the graph loop's condition.
+// NPT nodes per thread, blockDim.x apart along x (independent loads in flight per thread).
+template <typename S, int NPT>
 __global__ void __launch_bounds__(256) k_cg_pass_b(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,
                                                    const S *u0, const S *u1, const S *lap, double *partials,
                                                    CgState *cs, unsigned *counter, double *history,
@@ -693,16 +694,23 @@ __global__ void __launch_bounds__(256) k_cg_pass_b(Mesh m, int off, int gx, int 
   if (cs->done) return;                  // (host-driven iterations past convergence)
   const S *u = (cs->it & 1) ? u0 : u1;   // the direction pass A of this iteration wrote
   const S alpha = (S)cs->alpha;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
+  const int ix0 = blockIdx.x * blockDim.x * NPT + threadIdx.x + off;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
   double rr = 0.0;
-  if (ix < gx + off && iy < gy + off && iz < gz + off) {
-    const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
-    phi[idx] = phi[idx] + alpha * u[idx];
-    const S rn = r[idx] + (-alpha) * lap[idx];
-    r[idx] = rn;
-    rr = (double)rn * (double)rn;
+  if (iy < gy + off && iz < gz + off) {
+    const long long row = (long long)m.nx * (iy + (long long)m.ny * iz);
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int ix = ix0 + k * (int)blockDim.x;
+      if (ix < gx + off) {
+        const long long idx = ix + row;
+        phi[idx] = phi[idx] + alpha * u[idx];
+        const S rn = r[idx] + (-alpha) * lap[idx];
+        r[idx] = rn;
+        rr += (double)rn * (double)rn;
+      }
+    }
   }
   if (block_partial_and_ticket(rr, partials, counter)) {
     const int np = gridDim.x * gridDim.y * gridDim.z;

@@ -686,6 +686,30 @@ def test_cg_host_loop_equals_graph_loop():
     np.testing.assert_array_equal(out[0][2], out[1][2])
 
 
+def test_cg_on_a_grid_beyond_65536_blocks_runs_and_reduces_the_divergence():
+    # 290^3 (a 288^3 CG interior: 93,312 blocks of the pointwise pass, more than the 65,536
+    # partials the reduction buffers held before they were sized from the grid): the graph
+    # loop and the host loop give the same fields, and the residual falls
+    c = dict(order=4, testcase="confined_domain", nodes=(290, 290, 290), lo=0.0, hi=1.0,
+             laplace="WIDE_STENCIL_DIRICHLET", bnodes=1)
+    out = []
+    for loop in ("GRAPH", "HOST"):
+        m = maps_for(c)
+        m.I_Tech["cg_loop"] = loop
+        ctx = m.context()
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b)
+        bh[: ctx.n, :3] += NOISE_AMPLITUDE * np.random.default_rng(NOISE_SEED).random((ctx.n, 3))
+        db = ctx.vec(bh)
+        res = ctx.clean_div(db, 12, 1e-30, check=False)
+        out.append((res["iterations"], res["residual_norm2"], res["divergence_norm_initial"], ctx.get_vec(db)))
+        ctx.close()
+    assert out[0][0] == out[1][0] == 12 and out[0][1] == out[1][1]
+    assert out[0][1] < 1e-2 * out[0][2] ** 2
+    np.testing.assert_array_equal(out[0][3], out[1][3])
+
+
 FLUX_FORMS = [(ui, so, uj) for ui in ("CENTRAL", "SPLIT", "PRODUCT") for so in ("ZERO", "CENTRAL", "SPLIT")
               for uj in ("CENTRAL", "SPLIT", "PRODUCT")]
 
