@@ -174,11 +174,92 @@ def initialize(maps: Maps, u_max: float | None = None, device: int = 0):
     return ctx
 
 
-def compute_numerical_solution(ctx: Context, b, u, rho, num_steps: int, t_final: float) -> dict:
-    """compute_numerical_solution.m: the step loop (fused, graph captured) and the results."""
+def compute_numerical_solution(ctx: Context, b, u, rho, num_steps: int, t_final: float,
+                               save_integrals_over_time: bool = False, dc: dict | None = None) -> dict:
+    """compute_numerical_solution.m: the step loop (fused, graph captured) and the results
+    (I_Results: runtime, abs_err, rel_err, divergence_norm, energy; lines 197-250).
+
+    save_integrals_over_time (lines 153-173): energy, ||div B|| and the L2 error of B before
+    every step, with the final values appended (num_steps + 1 entries each, as
+    energy_over_time, L2error_divB_over_time, L2error_B_over_time) and the times
+    linspace(0, t_final, num_steps + 1).  dc: the I_DC map; with divergence_cleaning B is
+    cleaned after every step (lines 121-129) by the CG of clean_div.m with its
+    absolute_error_threshold and max_iterations.  Series and cleaning stay on the device
+    (ieq_time_steps_integrals)."""
+    import time as _time
     b2, b3, cb = ctx.vec(), ctx.vec(), ctx.vec()
-    time = ctx.scalar(np.zeros(2), n=2)
-    ctx.time_steps(b, b2, b3, cb, u, rho, time, num_steps)
+    clock = ctx.scalar(np.zeros(2), n=2)
+    clean = bool(dc and dc.get("divergence_cleaning"))
+    t0 = _time.perf_counter()
+    series = None
+    if save_integrals_over_time or clean:
+        series = ctx.time_steps_integrals(b, b2, b3, cb, u, rho, clock, num_steps,
+                                          int(dc["max_iterations"]) if clean else 0,
+                                          float(dc["absolute_error_threshold"]) if clean else 0.0)
+    else:
+        ctx.time_steps(b, b2, b3, cb, u, rho, clock, num_steps)
     ctx.synchronize()
+    runtime = _time.perf_counter() - t0
     wv, ws = ctx.vec(), ctx.scalar()
-    return ctx.results(b, t_final, wv, ws)
+    res = ctx.results(b, t_final, wv, ws)
+    res["runtime"] = runtime
+    if save_integrals_over_time:
+        res["energy_over_time"] = np.append(series["energy"], res["energy"])
+        res["L2error_divB_over_time"] = np.append(series["divergence_norm"], res["divergence_norm"])
+        res["L2error_B_over_time"] = np.append(series["l2_error"], res["abs_err"])
+        res["time"] = np.linspace(0.0, t_final, num_steps + 1)
+    return res
+
+
+def clean_div(ctx: Context, b, dc: dict) -> dict:
+    """clean_div.m: the CG projection of B with I_DC's absolute_error_threshold and
+    max_iterations (iterations, final residual, divergence_norm_initial)."""
+    return ctx.clean_div(b, int(dc["max_iterations"]), float(dc["absolute_error_threshold"]), check=False)
+
+
+# ---------------------------------------------------------------- time-series output
+# The paper scripts write the series of a run to an HDF5 file (paper/divcleaning_confined_domain.m
+# :183-190: datasets /time, /energy, /L2error_B, /L2error_divB) and one summary line per run
+# (:197-199).  The same datasets go to an .npz archive here (no HDF5 library is needed).
+
+SERIES_DATASETS = (("time", "time"), ("energy", "energy_over_time"), ("L2error_B", "L2error_B_over_time"),
+                   ("L2error_divB", "L2error_divB_over_time"))
+_DC_LABELS = {"USE_LAPLACE_WIDE_STENCIL_LNS": "WS_LN", "USE_LAPLACE_WIDE_STENCIL_DIRICHLET": "WS_D0",
+              "USE_LAPLACE_NARROW_STENCIL_DIRICHLET": "NS_D0"}
+
+
+def series_filename(maps: Maps, ext: str = ".npz") -> str:
+    """The paper script's file name of a run (divcleaning_confined_domain.m:162-177) with the
+    testcase as prefix: <testcase>_N_<N>_order_<p>_<uibj>_<source>_<ujbi>__DC_<0|1>[_<label>]."""
+    ieq, dc = maps.I_IEq, maps.I_DC
+    forms = "_".join(ieq[k].split("_", 2)[2].lower() for k in ("form_uibj", "form_source", "form_ujbi"))
+    name = f"{maps.I_RunOps['testcase']}_N_{int(maps.I_Mesh['NODES_X'])}_order_{int(maps.I_RunOps['order'])}_{forms}"
+    if dc.get("divergence_cleaning"):
+        name += "__DC_1_" + _DC_LABELS[dc["divergence_cleaning_form"]]
+    else:
+        name += "__DC_0"
+    return name + ext
+
+
+def write_series(path: str, results: dict) -> None:
+    """The series of a run (compute_numerical_solution with save_integrals_over_time) as an
+    .npz archive with the paper's dataset names (time, energy, L2error_B, L2error_divB),
+    float64; an existing file is replaced."""
+    np.savez(path, **{ds: np.asarray(results[key], dtype=np.float64) for ds, key in SERIES_DATASETS})
+
+
+def read_series(path: str) -> dict:
+    with np.load(path) as z:
+        return {ds: z[ds].copy() for ds, _ in SERIES_DATASETS}
+
+
+def summary_row(maps: Maps, results: dict) -> str:
+    """The paper script's summary line of a run (divcleaning_confined_domain.m:192-199): N,
+    order, the three flux forms, runtime, energy, abs_err, divergence_norm, the cleaning switch
+    and its form."""
+    ieq, dc = maps.I_IEq, maps.I_DC
+    on = bool(dc.get("divergence_cleaning"))
+    return "%d, %d, %s, %s, %s, %.15e, %.15e, %.15e, %.15e, %d, %s \n" % (
+        int(maps.I_Mesh["NODES_X"]), int(maps.I_RunOps["order"]), ieq["form_uibj"], ieq["form_source"],
+        ieq["form_ujbi"], results["runtime"], results["energy"], results["abs_err"], results["divergence_norm"],
+        int(on), dc["divergence_cleaning_form"] if on else " ")

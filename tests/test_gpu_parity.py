@@ -497,6 +497,50 @@ def test_time_steps_integrals_with_cleaning_match_oracle():
     assert rel_err(ctx.get_vec(dev[0]), host[0]) <= 1e-10
 
 
+@pytest.mark.parametrize("clean", [False, True])
+def test_compute_numerical_solution_series_and_results(clean, tmp_path):
+    # compute_numerical_solution with save_integrals_over_time (compute_numerical_solution.m
+    # :153-250): num_steps + 1 entries per series, the last being the final results, the
+    # others the device series of ieq_time_steps_integrals; written and read back as .npz
+    from inductioneq_b200.induction_eq import compute_numerical_solution, read_series, write_series
+    c = dict(order=4, testcase="confined_domain", nodes=(14, 15, 16), lo=0.0, hi=1.0, hall=True,
+             integrator="CarpenterKennedy2N54", dt=2e-4, laplace="WIDE_STENCIL_DIRICHLET", bnodes=1)
+    dc = {"divergence_cleaning": clean, "absolute_error_threshold": 1e-9, "max_iterations": 60}
+    steps = 3
+    out = []
+    for direct in (False, True):
+        m = maps_for(c)
+        ctx = m.context()
+        b = ctx.vec()
+        ctx.kernel("init_b", b)
+        bh = ctx.get_vec(b)
+        bh[: ctx.n, :3] += NOISE_AMPLITUDE * np.random.default_rng(NOISE_SEED).random((ctx.n, 3))
+        b.upload(bh)
+        u, rho = ctx.vec(), ctx.scalar(np.ones(ctx.n_pad))
+        if direct:
+            dev = [b, ctx.vec(), ctx.vec(), ctx.vec(), u, rho, ctx.scalar(np.zeros(2), n=2)]
+            ser = ctx.time_steps_integrals(*dev, steps, clean_max_iterations=60 if clean else 0,
+                                           clean_threshold=1e-9 if clean else 0.0)
+            fin = ctx.results(b, steps * 2e-4, ctx.vec(), ctx.scalar())
+            out.append((ser, fin))
+        else:
+            out.append(compute_numerical_solution(ctx, b, u, rho, steps, steps * 2e-4, save_integrals_over_time=True,
+                                                  dc=dc))
+        ctx.close()
+    res, (ser, fin) = out
+    for key, s_key, f_key in (("energy_over_time", "energy", "energy"),
+                              ("L2error_divB_over_time", "divergence_norm", "divergence_norm"),
+                              ("L2error_B_over_time", "l2_error", "abs_err")):
+        assert res[key].shape == (steps + 1,)
+        np.testing.assert_array_equal(res[key][:steps], ser[s_key])
+        assert res[key][steps] == fin[f_key] == res[f_key]
+    np.testing.assert_array_equal(res["time"], np.linspace(0.0, steps * 2e-4, steps + 1))
+    path = tmp_path / "series.npz"
+    write_series(str(path), res)
+    back = read_series(str(path))
+    np.testing.assert_array_equal(back["L2error_divB"], res["L2error_divB_over_time"])
+
+
 @pytest.mark.parametrize("integrator", ["SSPRK33", "SSPRK104", "KennedyCarpenterLewis2R54C", "CalvoFrancoRandez2R64",
                                         "CarpenterKennedy2N54", "ToulorgeDesmet2N84F"])
 @pytest.mark.parametrize("real", ["double", "float"])
