@@ -233,10 +233,11 @@ ieq_status ieq_batch_test_barrier(ieq_batch *batch, int extra_arrivals, long lon
 /* ---------------------------------------------------------------- discrete adjoint */
 
 /* Hand-written discrete adjoint of the spatial operator F(b) = DB (volume terms, Hall term
- * with J = curl(b)/rho, high-order dissipation, inflow SAT) at fixed u and rho, and of the
- * SSPRK33 step.  No counterpart in the reference.  FP64 only; Hall runs must be periodic (the
- * Hall outflow SAT switches on the sign of 0.5u - J and has no adjoint); first-order and
- * adaptive dissipation are not supported.  Vector fields in the reference layout. */
+ * with J = curl(b)/rho, high-order and first-order dissipation, inflow SAT, Hall outflow SAT)
+ * at fixed u and rho, and of the SSPRK33 and 2N steps.  No counterpart in the reference.
+ * FP64 only.  The Hall outflow SAT switches on the sign of 0.5u - J: it is differentiated with
+ * the switch held (its derivative away from tv = 0).  Adaptive dissipation (weights that depend
+ * on b) returns IEQ_ERR_SETTINGS.  Vector fields in the reference layout. */
 /* out = F'(b) v (tangent linear) */
 ieq_status ieq_operator_jvp(ieq_ctx *ctx, const void *b, const void *v, const void *u, const void *rho,
                             void *out);

@@ -12,8 +12,9 @@
 //   kernels of the time stepping with the stage states written out per stage
 // The transposes are written out per term (see the notes at k_vjp_pass1); D^T is applied as
 // a gather over the neighbours j = k + p with the coefficient of row(j) at offset -p.
-// The Hall outflow SAT (a switch on the sign of 0.5u - J) has no adjoint here: Hall runs
-// must be periodic.
+// The Hall outflow SAT (a switch on the sign of 0.5u - J) is differentiated away from the
+// switch (tv_a = 0); first-order dissipation is linear in b at fixed u; adaptive dissipation
+// (weights that depend on b through a square root and thresholds) has no adjoint.
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -29,7 +30,7 @@ struct AdjArgs {
   Mesh m;
   const Tables<double> *tab;
   int nb, sw, wh, periodic;
-  int conv, hall, hod;
+  int conv, hall, hod, fo;   // fo: first-order dissipation (linear in b at fixed u)
   double hod_factor;
   double w[6];           // flux-form weights (see stage_kernel.cuh)
   double inv_d[3], two_inv_d[3], sat_s[3];
@@ -140,6 +141,63 @@ __device__ __forceinline__ bool make_node(const AdjArgs &a, Node &nd) {
   return true;
 }
 
+// first-order dissipation (artificial_dissipation.cl:36-80) along ax, linear in b at fixed u:
+// forward  sum_o |D[row k][o]| sigma(u_{k+o}, u_k) (x_{k+o} - x_k)
+// transpose sum_p |D[row (k+p)][-p]| sigma(u_k, u_{k+p}) x_{k+p} - (sum_o |D[row k][o]| sigma(u_{k+o}, u_k)) x_k
+// (sigma: the componentwise larger |u|; the caller multiplies by 1/d)
+__device__ __forceinline__ V3<double> sigma3(V3<double> p, V3<double> q) {
+  return {fmax(fabs(p.x), fabs(q.x)), fmax(fabs(p.y), fabs(q.y)), fmax(fabs(p.z), fabs(q.z))};
+}
+template <bool TR>
+__device__ V3<double> fo_apply(const AdjArgs &a, const Node &nd, int ax, const R4<double> *x) {
+  const int c0 = (a.sw - 1) / 2;
+  const int rk = row_of(a, nd.i[ax], nd.n[ax]);
+  const V3<double> uk = ld(a.u, nd.idx), xk = ld(x, nd.idx);
+  V3<double> s = {0, 0, 0}, diag = {0, 0, 0};
+  for (int o = -c0; o <= c0; ++o) {
+    long long j;
+    int jj;
+    if (!nbr_idx(a, nd, ax, o, j, jj)) continue;
+    const V3<double> uj = ld(a.u, j);
+    const double cf = fabs(a.tab->D[rk][o + c0]);
+    if (!TR) {
+      if (cf == 0.0) continue;
+      const V3<double> sg = sigma3(uj, uk), xj = ld(x, j);
+      s.x += cf * sg.x * (xj.x - xk.x);
+      s.y += cf * sg.y * (xj.y - xk.y);
+      s.z += cf * sg.z * (xj.z - xk.z);
+    } else {
+      const V3<double> sg = sigma3(uj, uk);
+      if (cf != 0.0) diag = {diag.x + cf * sg.x, diag.y + cf * sg.y, diag.z + cf * sg.z};
+      const double ct = fabs(a.tab->D[row_of(a, jj, nd.n[ax])][c0 - o]);
+      if (ct == 0.0) continue;
+      const V3<double> xj = ld(x, j);
+      s.x += ct * sg.x * xj.x;
+      s.y += ct * sg.y * xj.y;
+      s.z += ct * sg.z * xj.z;
+    }
+  }
+  if (TR) s = {s.x - diag.x * xk.x, s.y - diag.y * xk.y, s.z - diag.z * xk.z};
+  return s;
+}
+
+// The Hall outflow SAT at a boundary node (induction_Eq_surface.cl:35-81), per face axis a
+// with c = M_INV[0]/d_a, tv = 0.5 u - J (J = curl(b)/rho), sw = -[left, tv_a > 0] + [right,
+// tv_a < 0], side = -[left] + [right]:  S = c (sw tv_a b + side b_a J).  Away from tv_a = 0
+// its tangent is  c (sw (tv_a v - dJ_a b) + side (v_a J + b_a dJ)),  dJ = curl(v)/rho.
+struct HallSat {
+  double c, tva, sw, side;
+};
+__device__ __forceinline__ bool hall_sat_axis(const AdjArgs &a, const Node &nd, int ax, V3<double> tv, HallSat &h) {
+  const bool l = nd.i[ax] == 0, r = nd.i[ax] == nd.n[ax] - 1;
+  if (!l && !r) return false;
+  h.c = a.sat_s[ax];
+  h.tva = comp(tv, ax);
+  h.sw = (l && h.tva > 0 ? -1.0 : 0.0) + (r && h.tva < 0 ? 1.0 : 0.0);
+  h.side = (l ? -1.0 : 0.0) + (r ? 1.0 : 0.0);
+  return true;
+}
+
 // SAT of the inflow boundary (induction_Eq_surface.cl:7-33): linear in b with the diagonal
 // coefficient sum_a s_a c_a u_a on the faces
 __device__ double sat_diag(const AdjArgs &a, const Node &nd, V3<double> um) {
@@ -194,8 +252,21 @@ __global__ void k_jvp(const AdjArgs a) {
       out = axpy3(a.inv_d[ax], s, out);
     }
     if (a.hod) out = axpy3(a.hod_factor, hod_apply<false>(a, nd, ax, a.v), out);
+    if (a.fo) out = axpy3(a.inv_d[ax], fo_apply<false>(a, nd, ax, a.v), out);
   }
   out = axpy3(sat_diag(a, nd, um), vm, out);
+  if (a.hall && !a.periodic) {
+    const V3<double> b0 = ld(a.b0, k), J0 = ld(a.J0, k), dJ = ld(a.dJ, k);
+    const V3<double> tv = {0.5 * um.x - J0.x, 0.5 * um.y - J0.y, 0.5 * um.z - J0.z};
+    for (int ax = 0; ax < 3; ++ax) {
+      HallSat h;
+      if (!hall_sat_axis(a, nd, ax, tv, h)) continue;
+      const double dJa = comp(dJ, ax), va = comp(vm, ax), ba = comp(b0, ax);
+      out.x += h.c * (h.sw * (h.tva * vm.x - dJa * b0.x) + h.side * (va * J0.x + ba * dJ.x));
+      out.y += h.c * (h.sw * (h.tva * vm.y - dJa * b0.y) + h.side * (va * J0.y + ba * dJ.y));
+      out.z += h.c * (h.sw * (h.tva * vm.z - dJa * b0.z) + h.side * (va * J0.z + ba * dJ.z));
+    }
+  }
   st3(a.out + k, out);
 }
 
@@ -331,6 +402,7 @@ __global__ void k_vjp_pass1(const AdjArgs a) {
       }
       pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
       if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+      if (a.fo) z = axpy3(a.inv_d[ax], fo_apply<true>(a, nd, ax, a.v), z);
     }
   } else {
     if (a.hall) J0m = ld(a.J0, k);
@@ -352,9 +424,24 @@ __global__ void k_vjp_pass1(const AdjArgs a) {
       }
       pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
       if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
+      if (a.fo) z = axpy3(a.inv_d[ax], fo_apply<true>(a, nd, ax, a.v), z);
     }
   }
   z = axpy3(sat_diag(a, nd, um), wm, z);
+  if (a.hall && !a.periodic) {
+    // transpose of the Hall outflow SAT's tangent: the terms in v at the node, and the source
+    // for dJ (transposed through the curl by pass 2 with the Hall volume term's)
+    const V3<double> tv = {0.5 * um.x - J0m.x, 0.5 * um.y - J0m.y, 0.5 * um.z - J0m.z};
+    const double bw = dot3(b0m, wm), Jw = dot3(J0m, wm);
+    for (int ax = 0; ax < 3; ++ax) {
+      HallSat h;
+      if (!hall_sat_axis(a, nd, ax, tv, h)) continue;
+      z = axpy3(h.c * h.sw * h.tva, wm, z);
+      addc(z, ax, h.c * h.side * Jw);
+      addc(gJ, ax, -h.c * h.sw * bw);
+      gJ = axpy3(h.c * h.side * comp(b0m, ax), wm, gJ);
+    }
+  }
   if (a.hall) {
     st3(a.out + k, z);
     const double r = 1.0 / a.rho[k];
@@ -435,6 +522,7 @@ AdjArgs adj_args(ieq_ctx *c) {
   a.conv = 1;
   a.hall = c->s.hall ? 1 : 0;
   a.hod = c->s.diss_form == 1 ? 1 : 0;
+  a.fo = c->s.diss_form == 2 ? 1 : 0;
   a.hod_factor = c->s.hod_factor;
   return a;
 }
@@ -449,9 +537,8 @@ ieq_status afail(ieq_ctx *c, ieq_status st, const std::string &m) {
 
 ieq_status check_adjoint_settings(ieq_ctx *c) {
   if (c->s.real_float) return afail(c, IEQ_ERR_SETTINGS, "the adjoint is FP64 only");
-  if (c->s.hall && !c->s.periodic) return afail(c, IEQ_ERR_SETTINGS, "the Hall outflow SAT has no adjoint: Hall runs must be periodic");
-  if (c->s.diss_form == 2 || c->s.diss_form == 3)
-    return afail(c, IEQ_ERR_SETTINGS, "first-order/adaptive dissipation has no adjoint");
+  if (c->s.diss_form == 3)
+    return afail(c, IEQ_ERR_SETTINGS, "adaptive dissipation (weights that depend on b) has no adjoint");
   if (c->s.uibj < 0 || c->s.source < 0 || c->s.ujbi < 0) return afail(c, IEQ_ERR_SETTINGS, "no flux forms");
   return IEQ_OK;
 }
@@ -512,7 +599,7 @@ ieq_status vjp(ieq_ctx *c, const void *b, const void *w, const void *u, const vo
   a.rho = (const double *)rho;
   a.out = (R4<double> *)out;
   a.gJr = (R4<double> *)gJr;
-  if (c->s.hall && fast_ri(c) == 0) {   // else pass 1 forms J0 at the node itself
+  if (c->s.hall && (!c->s.periodic || fast_ri(c) == 0)) {   // else pass 1 forms J0 at every node itself
     adj_curl(c, b, rho, J0);
     a.J0 = (const R4<double> *)J0;
   }

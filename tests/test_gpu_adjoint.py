@@ -6,7 +6,8 @@
 * the checkpointed SSPRK33 gradient of a final-time L2 misfit against central differences
   along seeded random directions (Richardson-extrapolated, relative 1e-6), driven through a torch.autograd.Function
   (defined here, in the test harness only);
-* the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F).
+* the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F), and for
+  Hall on boxes (the outflow SAT) and first-order dissipation.
 """
 from __future__ import annotations
 
@@ -30,13 +31,32 @@ CASES = {
     "rot3d_4e_split_hod": dict(order=4, extended=True, testcase="rotation_3D", nodes=(14, 13, 15), lo=-1.0, hi=1.0,
                                uibj="SPLIT", source="SPLIT", ujbi="PRODUCT", dissipation="HIGH_ORDER",
                                integrator="SSPRK33"),
+    # Hall on boxes: the Hall outflow SAT (induction_Eq_surface.cl:35-81) on every face
+    "travel_6c_hall_box": dict(order=6, testcase="hall_travelling_wave", nodes=(14, 15, 16), lo=0.0, hi=6.283185307179586,
+                               hall=True, integrator="SSPRK33"),
+    # (u . n = 0 on the walls and curl(B) . n = 0 on the box edges: the outflow switch sits at
+    # tv = 0 there, where it has no derivative; seeded noise on B moves the state off it)
+    "confined_4c_hall_fo": dict(order=4, testcase="confined_domain", nodes=(15, 14, 13), lo=0.0, hi=1.0, hall=True,
+                                dissipation="FIRST_ORDER", integrator="SSPRK33", noise=1e-2),
+    # first-order dissipation with convection only (its weights max(|u_j|, |u_k|) are fixed)
+    "rot_2c_fo": dict(order=2, testcase="rotation_gaussian", nodes=(13, 12, 11), lo=-1.0, hi=1.0,
+                      dissipation="FIRST_ORDER", integrator="SSPRK33"),
 }
+
+
+def _noisy(ctx, b, c):
+    """B plus the case's seeded noise (off the outflow switch's non-smooth points)."""
+    if c.get("noise"):
+        bh = ctx.get_vec(b)
+        bh[: ctx.n, :3] += c["noise"] * np.random.default_rng(23).standard_normal((ctx.n, 3))
+        b.upload(bh)
 
 
 def _setup(c, dt=1.0):
     ctx = maps_for(dict(c, dt=dt)).context()
     b, u = ctx.vec(), ctx.vec()
     ctx.kernel("init_b", b)
+    _noisy(ctx, b, c)
     ctx.kernel("init_u", u)
     rho = ctx.scalar(np.ones(ctx.n_pad))
     return ctx, b, u, rho
@@ -77,7 +97,7 @@ def ctx_nodes(ctx):
     return ctx._nodes
 
 
-@pytest.mark.parametrize("name", ["hallper_4c", "rot_6c_sat"])
+@pytest.mark.parametrize("name", ["hallper_4c", "rot_6c_sat", "travel_6c_hall_box", "confined_4c_hall_fo", "rot_2c_fo"])
 def test_tangent_matches_central_differences(name):
     c = dict(CASES[name], integrator="CarpenterKennedy2N54")
     ctx, b, u, rho = _setup(c)
@@ -266,6 +286,66 @@ def test_low_storage_step_adjoint_matches_central_differences(integrator):
             return (loss(b0 + e * d) - loss(b0 - e * d)) / (2 * e)
         rich = (4.0 * cd(5e-4) - cd(1e-3)) / 3.0
         assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["travel_6c_hall_box", "confined_4c_hall_fo"])
+def test_sweep_through_hall_boxes_matches_central_differences(name):
+    # the checkpointed SSPRK33 adjoint through steps with the Hall outflow SAT (and first-order
+    # dissipation) against Richardson-extrapolated central differences of the time stepping
+    c = CASES[name]
+    ctx = maps_for(dict(c, dt=1e-3)).context()
+    nsteps, every = 6, 4
+    b, u = ctx.vec(), ctx.vec()
+    ctx.kernel("init_b", b)
+    _noisy(ctx, b, c)
+    ctx.kernel("init_u", u)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    b0, u0 = ctx.get_vec(b), ctx.get_vec(u)
+    n = ctx.n
+    rng = np.random.default_rng(17)
+
+    def forward(x):
+        bb, b2, b3, cb, uu = ctx.vec(x), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(u0)
+        ctx.time_steps(bb, b2, b3, cb, uu, rho, ctx.scalar(np.zeros(2), n=2), nsteps)
+        return ctx.get_vec(bb)
+
+    target = forward(b0) + 1e-3 * rng.standard_normal((ctx.n_pad, 4))
+    target[:, 3] = 0
+    target[n:] = 0
+
+    def loss(x):
+        d = forward(x)[:n, :3] - target[:n, :3]
+        return 0.5 * float(np.sum(d * d))
+
+    g0 = np.zeros_like(b0)
+    g0[:n, :3] = forward(b0)[:n, :3] - target[:n, :3]
+    lam = ctx.vec(g0)
+    ctx.adjoint_steps(ctx.vec(b0), lam, ctx.vec(u0), rho, nsteps, every)
+    grad = ctx.get_vec(lam)
+    for k in range(3):
+        d = rng.standard_normal((ctx.n_pad, 4))
+        d[:, 3] = 0
+        d[n:] = 0
+        d /= np.sqrt(np.sum(d[:, :3] ** 2))
+        ad = float(np.sum(grad[:, :3] * d[:, :3]))
+
+        def cd(e):
+            return (loss(b0 + e * d) - loss(b0 - e * d)) / (2 * e)
+        # small steps: a larger one can carry a boundary node's tv_a across the outflow switch
+        # somewhere along the trajectory, where the loss has a kink
+        rich = (4.0 * cd(5e-7) - cd(1e-6)) / 3.0
+        assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
+    ctx.close()
+
+
+def test_adjoint_of_adaptive_dissipation_is_refused():
+    c = dict(CASES["rot_2c_fo"], dissipation="ADAPTIVE")
+    ctx = maps_for(dict(c, dt=1e-3)).context()
+    from inductioneq_b200.lib import IeqError
+    with pytest.raises(IeqError) as e:
+        ctx.operator_vjp(ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)), ctx.vec())
+    assert e.value.name == "IEQ_ERR_SETTINGS"
     ctx.close()
 
 
