@@ -162,15 +162,23 @@ __device__ V3<R> tc_rotation_3d_b(R x, R y, R z, R t) {
           ((1 - c - sqrt3 * s) * b0x + (1 - c + sqrt3 * s) * b0y + (1 + 2 * c) * b0z) / (R)3.0};
 }
 
-// include/hall_periodic.h:3-34 (b) and 75-92 (u)
+// include/hall_periodic.h:3-34 (b) and 75-92 (u).  u is a sum of one-dimensional terms,
+// u1 = c(y) + s(z), u2 = c(z) + s(x), u3 = c(x) + s(y) with c(q) = a cos(k q + al k t n),
+// s(q) = a sin(k q + al k t n)
 template <typename R>
-__device__ V3<R> tc_hall_periodic_u(R x, R y, R z, R t) {
+__device__ __forceinline__ void tc_hall_periodic_terms(R q, R t, R &c, R &s) {
   const R n = (R)0.5773502691896258, a = (R)1, al = (R)0.5;
   const R k = (R)(1.0 - al * al) / al;
-  R u1 = a * cos(k * y + al * k * t * n) + a * sin(k * z + al * k * t * n);
-  R u2 = a * cos(k * z + al * k * t * n) + a * sin(k * x + al * k * t * n);
-  R u3 = a * cos(k * x + al * k * t * n) + a * sin(k * y + al * k * t * n);
-  return {u1, u2, u3};
+  c = a * cos(k * q + al * k * t * n);
+  s = a * sin(k * q + al * k * t * n);
+}
+template <typename R>
+__device__ V3<R> tc_hall_periodic_u(R x, R y, R z, R t) {
+  R cx, sx, cy, sy, cz, sz;
+  tc_hall_periodic_terms(x, t, cx, sx);
+  tc_hall_periodic_terms(y, t, cy, sy);
+  tc_hall_periodic_terms(z, t, cz, sz);
+  return {cy + sz, cz + sx, cx + sy};
 }
 
 // include/hall_travelling_wave.h:3-30 (b) and 66-82 (u)

@@ -22,8 +22,42 @@ __device__ __forceinline__ void st_any(R *base, long long vstride, long long idx
   }
 }
 
+// u of hall_periodic at time t (a sum of one-dimensional terms): the block evaluates the
+// terms once per x, y and z index of its tile in shared memory (blockDim.x + y + z cosine and
+// sine pairs instead of six per node), then adds them per node
+template <typename R>
+__device__ void hall_periodic_u_block(const Mesh &m, R *vout, long long vstride, R t) {
+  __shared__ R tc[3][32], ts[3][32];   // [axis][index within the tile]
+  const int dim[3] = {(int)blockDim.x, (int)blockDim.y, (int)blockDim.z};
+  const int base[3] = {(int)(blockIdx.x * blockDim.x), (int)(blockIdx.y * blockDim.y), (int)(blockIdx.z * blockDim.z)};
+  const int lin = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  int ax = -1, k = lin;
+  for (int a = 0; a < 3 && ax < 0; ++a) {
+    if (k < dim[a]) ax = a;
+    else k -= dim[a];
+  }
+  if (ax >= 0) {
+    int ii[3] = {0, 0, 0};
+    ii[ax] = base[ax] + k;
+    R q[3];
+    coords<R>(m, ii[0], ii[1], ii[2], q[0], q[1], q[2]);
+    tc_hall_periodic_terms(q[ax], t, tc[ax][k], ts[ax][k]);
+  }
+  __syncthreads();
+  const int ix = base[0] + threadIdx.x, iy = base[1] + threadIdx.y, iz = base[2] + threadIdx.z;
+  if (ix >= m.nx || iy >= m.ny || iz >= m.nz) return;
+  const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
+  const int x = threadIdx.x, y = threadIdx.y, z = threadIdx.z;
+  st_any(vout, vstride, idx, V3<R>{tc[1][y] + ts[2][z], tc[2][z] + ts[0][x], tc[0][x] + ts[1][y]});
+}
+
 template <typename R>
 __global__ void k_init(Mesh m, int tc, int kind, R *vout, long long vstride, R *sout, const R *time) {
+  if (kind == CALC_U && tc == TC_HALL_PERIODIC && blockDim.x <= 32 && blockDim.y <= 32 && blockDim.z <= 32 &&
+      blockDim.x * blockDim.y * blockDim.z >= blockDim.x + blockDim.y + blockDim.z) {
+    hall_periodic_u_block<R>(m, vout, vstride, time[1]);
+    return;
+  }
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z * blockDim.z + threadIdx.z;
