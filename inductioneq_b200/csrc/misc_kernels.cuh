@@ -378,19 +378,6 @@ struct CgState {
   int pad;
 };
 
-// u = beta*u + r with beta = rr/old (calc_axpy over the I_DC g_range)
-template <typename S>
-__global__ void k_cg_direction(Mesh m, int off, int gx, int gy, int gz, S *u, const S *r, const CgState *cs) {
-  if (cs->done) return;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
-  if (ix >= gx + off || iy >= gy + off || iz >= gz + off) return;
-  const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
-  const S beta = (S)(cs->rr / cs->old);
-  u[idx] = beta * u[idx] + r[idx];
-}
-
 // sum of np partials in a fixed order by the calling block (all threads get the total)
 __device__ __forceinline__ double block_sum_partials(const double *partials, int np) {
   __shared__ double sm[32];
@@ -433,102 +420,16 @@ __device__ __forceinline__ bool block_partial_and_ticket(double v, double *parti
   return last;
 }
 
-// lap = (-Laplace) u over the interior; alpha = rr / <u, lap> (last block)
-template <typename S>
-__global__ void __launch_bounds__(256) k_cg_laplace(const LapArgs<S> a, CgState *cs, unsigned *counter) {
-  if (cs->done) return;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
-  double prod = 0.0;
-  if (ix < a.gx + a.off && iy < a.gy + a.off && iz < a.gz + a.off) {
-    const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
-    const S val = laplace_at(a, ix, iy, iz, idx);
-    a.out[idx] = val;
-    prod = (double)a.in[idx] * (double)val;
-  }
-  if (block_partial_and_ticket(prod, a.partials, counter)) {
-    const int np = gridDim.x * gridDim.y * gridDim.z;
-    const double ul = block_sum_partials(a.partials, np);
-    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-      cs->alpha = cs->rr / ul;
-      *counter = 0u;
-    }
-  }
-}
-
 // The same operator for the device-resident CG loop, with the row width W fixed at compile
 // time and the coefficients pre-divided by DX^2, DY^2, DZ^2 (Ls[axis][row][c] = L[row][c] /
 // dd[axis]; Li: the interior row of each axis): a multiply per term instead of the
 // reference's division (cf * u) / dd.  Every term differs from the reference's by at most
-// a rounding of the scaled coefficient; the sum runs in the reference's order.  Nodes whose
-// three rows are interior (boxes) take unrolled loads at fixed offsets.
+// a rounding of the scaled coefficient; the sum runs in the reference's order.
 template <int W>
 struct LapFastArgs {
   double Li[3][W];
   const double *Ls;   // [3][2nb+1][W]
 };
-template <int W>
-__device__ __forceinline__ double laplace_fast_at(const LapArgs<double> &a, const LapFastArgs<W> &f, int ix, int iy,
-                                                  int iz, long long idx) {
-  constexpr int C0 = (W - 1) / 2;
-  const int ii[3] = {ix, iy, iz};
-  const int nn[3] = {a.m.nx, a.m.ny, a.m.nz};
-  const long long st[3] = {1, a.m.nx, (long long)a.m.nx * a.m.ny};
-  int row[3];
-#pragma unroll
-  for (int ax = 0; ax < 3; ++ax) row[ax] = a.periodic ? a.nb : sbp_row(ii[ax], nn[ax], a.nb);
-  double val = 0;
-  if (!a.periodic && row[0] == a.nb && row[1] == a.nb && row[2] == a.nb) {
-#pragma unroll
-    for (int c = 0; c < W; ++c) {
-      double t[3];
-#pragma unroll
-      for (int ax = 0; ax < 3; ++ax) t[ax] = __ldg(a.in + idx + (long long)(c - C0) * st[ax]) * f.Li[ax][c];
-      val = ((val + t[0]) + t[1]) + t[2];
-    }
-    return val;
-  }
-  const int rows = 2 * a.nb + 1;
-#pragma unroll
-  for (int c = 0; c < W; ++c) {
-    double t[3];
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-      const double cf = f.Ls[(ax * rows + row[ax]) * W + c];
-      const long long j = idx + (long long)(nbr_rt<double>(ii[ax], c - C0, nn[ax], a.periodic) - ii[ax]) * st[ax];
-      t[ax] = a.in[j] * cf;
-    }
-    val = ((val + t[0]) + t[1]) + t[2];
-  }
-  return val;
-}
-
-// lap = (-Laplace) u over the interior; alpha = rr / <u, lap> (last block)
-template <int W>
-__global__ void __launch_bounds__(256) k_cg_laplace_fast(const LapArgs<double> a, const LapFastArgs<W> f, CgState *cs,
-                                                         unsigned *counter) {
-  if (cs->done) return;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + a.off;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y + a.off;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z + a.off;
-  double prod = 0.0;
-  if (ix < a.gx + a.off && iy < a.gy + a.off && iz < a.gz + a.off) {
-    const long long idx = ix + (long long)a.m.nx * (iy + (long long)a.m.ny * iz);
-    const double val = laplace_fast_at<W>(a, f, ix, iy, iz, idx);
-    a.out[idx] = val;
-    prod = a.in[idx] * val;
-  }
-  if (block_partial_and_ticket(prod, a.partials, counter)) {
-    const int np = gridDim.x * gridDim.y * gridDim.z;
-    const double ul = block_sum_partials(a.partials, np);
-    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-      cs->alpha = cs->rr / ul;
-      *counter = 0u;
-    }
-  }
-}
-
 // ---- the two passes of one CG iteration inside a graph loop (a conditional WHILE node
 // whose condition the last block of pass B sets; no host round trip per iteration).
 //
@@ -784,50 +685,6 @@ static __global__ void k_cg_start_loop(const double *partials_rr, int np, CgStat
     if (history) history[0] = rr;
     cs->done = !(rr > cs->tol && cs->it < cs->max_it);
     if (in_loop) cudaGraphSetConditional(loop, cs->done ? 0u : 1u);
-  }
-}
-
-// phi += alpha*u; r -= alpha*lap; rr = <r, r> (last block), then the loop condition
-template <typename S>
-__global__ void __launch_bounds__(256) k_cg_update(Mesh m, int off, int gx, int gy, int gz, S *phi, S *r,
-                                                   const S *u, const S *lap, double *partials, CgState *cs,
-                                                   unsigned *counter, double *history) {
-  if (cs->done) return;
-  const S alpha = (S)cs->alpha;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x + off;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y + off;
-  const int iz = blockIdx.z * blockDim.z + threadIdx.z + off;
-  double rr = 0.0;
-  if (ix < gx + off && iy < gy + off && iz < gz + off) {
-    const long long idx = ix + (long long)m.nx * (iy + (long long)m.ny * iz);
-    phi[idx] = phi[idx] + alpha * u[idx];
-    const S rn = r[idx] + (-alpha) * lap[idx];
-    r[idx] = rn;
-    rr = (double)rn * (double)rn;
-  }
-  if (block_partial_and_ticket(rr, partials, counter)) {
-    const int np = gridDim.x * gridDim.y * gridDim.z;
-    const double tot = block_sum_partials(partials, np);
-    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-      cs->old = cs->rr;
-      cs->rr = tot;
-      cs->it += 1;
-      if (history) history[cs->it] = tot;
-      cs->done = !(tot > cs->tol && cs->it < cs->max_it);
-      *counter = 0u;
-    }
-  }
-}
-
-// initial residual r = div B: rr = <r, r> from reduction partials, and the loop condition
-static __global__ void k_cg_start(const double *partials_rr, int np, CgState *cs, double *history) {
-  const double rr = block_sum_partials(partials_rr, np);
-  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-    cs->rr = rr;
-    cs->old = 1.0;
-    cs->it = 0;
-    if (history) history[0] = rr;
-    cs->done = !(rr > cs->tol && cs->it < cs->max_it);
   }
 }
 
