@@ -497,6 +497,34 @@ def test_time_steps_integrals_with_cleaning_match_oracle():
     assert rel_err(ctx.get_vec(dev[0]), host[0]) <= 1e-10
 
 
+@pytest.mark.parametrize("diss", ["FIRST_ORDER", "ADAPTIVE"])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_first_order_and_adaptive_dissipation_with_zero_velocity(diss, periodic):
+    # with u = 0 the fused path runs first-order dissipation as no dissipation and the
+    # adaptive form as the high-order dissipation (every kappa is 0); against the oracle's full
+    # formulas (artificial_dissipation.cl:36-160) and the reference kernel lists
+    c = dict(order=6, testcase="hall_circular_wave", nodes=(12, 13, 14), lo=0.0, hi=TWO_PI_, periodic=periodic,
+             hall=True, dissipation=diss, integrator="CarpenterKennedy2N54", dt=0.005)
+    o = oracle_for(c)
+    b = o.vec()
+    o.run("init_b", o.cfg.nodes, b)
+    b[:, :3] += 1e-2 * np.random.default_rng(NOISE_SEED).standard_normal((o.N, 3))
+    steps = 2
+    host = [b.copy(), o.vec(), o.vec(), o.vec(), o.vec(), o.scalar(fill=1.0), np.zeros(2)]
+    time_loop(o, c["integrator"], True, False, steps, host[0], host[1], None, host[3], host[4], host[5], host[6])
+    mb = float(np.abs(host[0]).max())
+    for kernel in ("AUTO", "LIST"):
+        ctx = maps_for(dict(c, stage_kernel=kernel)).context()
+        dev = [ctx.vec(b), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)),
+               ctx.scalar(np.zeros(2), n=2)]
+        ctx.time_steps(*dev, steps)
+        for i, kind in ((0, None), (1, "register")):
+            fl = rounding_floor(c, kind, mb, 0.0, stages_of(c, steps)) if kind else 0.0
+            ok, e = field_ok(ctx.get_vec(dev[i]), host[i], TOL64, fl)
+            assert ok, (kernel, i, e)
+        ctx.close()
+
+
 @pytest.mark.parametrize("clean", [False, True])
 def test_compute_numerical_solution_series_and_results(clean, tmp_path):
     # compute_numerical_solution with save_integrals_over_time (compute_numerical_solution.m
