@@ -348,9 +348,10 @@ def sharded_batch(rk, dev, steps=200, reps=3):
 
 def decomposed_solve(rk, dev, n=128, steps=4, reps=3):
     """One whistler solve (6th order + HOD, Hall, CK2N54, FP64, periodic n^3) decomposed into
-    z slabs over the ranks (inductioneq_b200.decomp: each rank runs the reference kernel lists
-    on its slab, ghost planes exchanged between kernels through NCCL); value = the solve's
-    DOF-updates / max-over-ranks time (strong scaling: the grid is fixed)."""
+    z slabs over the ranks (inductioneq_b200.decomp: each rank runs the fused stage kernels on
+    its slab one RK stage at a time, ghost planes exchanged between stages through NCCL; the
+    reference kernel lists with an exchange after every kernel are timed beside it); value =
+    the solve's DOF-updates / max-over-ranks time (strong scaling: the grid is fixed)."""
     import numpy as np
     import torch
 
@@ -365,21 +366,26 @@ def decomposed_solve(rk, dev, n=128, steps=4, reps=3):
     g.kernel("init_b", b)
     b0 = g.get_vec(b)[: g.n]
     g.close()
-    s.load(b0, None, np.ones(n ** 3))
-    s.steps(1)   # warm
-    times = []
-    for _ in range(reps):
+    def timed(fused):
         s.load(b0, None, np.ones(n ** 3))
-        R.barrier(rk)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        s.steps(steps)
-        times.append(time.perf_counter() - t0)
-    t = R.max_over_ranks(rk, statistics.median(times), device="cuda")
+        s.steps(1, fused=fused)   # warm
+        times = []
+        for _ in range(reps):
+            s.load(b0, None, np.ones(n ** 3))
+            R.barrier(rk)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            s.steps(steps, fused=fused)
+            times.append(time.perf_counter() - t0)
+        return R.max_over_ranks(rk, statistics.median(times), device="cuda")
+
+    t = timed(True)
+    t_lists = timed(False)
     s.close()
     return {"metric": METRIC + " (one solve decomposed into z slabs)", "value": 3 * n ** 3 * STAGES * steps / t,
             "unit": "DOF/s", "n_gpus": rk.world, "ms_per_rk_step": t / steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "dtype": "f64", "data": "synthetic (analytic whistler wave)",
+            "kernel_lists": {"value": 3 * n ** 3 * STAGES * steps / t_lists, "ms_per_rk_step": t_lists / steps * 1e3},
             "config": {"workload": f"hall_circular_wave {n}^3 periodic, 6th order + HOD, CK2N54, decomposed into "
                                    f"{rk.world} z slabs", "ghost_planes": s.slabs.ghosts,
                        "timing": "host clock around the steps (the kernels of a slab and its exchanges are "

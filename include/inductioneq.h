@@ -230,6 +230,28 @@ int ieq_batch_grid(const ieq_batch *batch);
  * production barrier; every run starts from a reset barrier state. */
 ieq_status ieq_batch_test_barrier(ieq_batch *batch, int extra_arrivals, long long spin_limit);
 
+/* ---------------------------------------------------------------- stage-by-stage stepping */
+
+/* The fused time step of ieq_time_steps enqueued one RK stage at a time, for a caller that
+ * acts between stages -- the z-slab decomposition of one solve over several GPUs refreshes
+ * the ghost planes of the state fields after every stage.  No counterpart in the reference
+ * (its host runs whole kernel lists).
+ *   ieq_stages_begin copies the fields (reference layout) into the context's fused state and
+ *     returns the stages of one step of the configured integrator;
+ *   ieq_stages_run enqueues stage `stage` (0 .. stages_per_step - 1, in order; after the last
+ *     stage the next stage 0 starts a new step) on the context's stream;
+ *   ieq_stages_field gives the state field `field` (0: b1, 1: b2, 2: b3 or db of the
+ *     three-field schemes) as it stands after the last stage run: the device address of its x
+ *     plane, the y and z planes following at component_stride elements (REAL); the fused path
+ *     alternates some fields between two buffers, so ask after every stage;
+ *   ieq_stages_end copies the state back into the fields.
+ * The fields may not be used by other calls on the context between begin and end. */
+ieq_status ieq_stages_begin(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u,
+                            int *stages_per_step);
+ieq_status ieq_stages_run(ieq_ctx *ctx, void *rho, void *time, int stage);
+ieq_status ieq_stages_field(ieq_ctx *ctx, int field, void **base, long long *component_stride);
+ieq_status ieq_stages_end(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB_rho, void *u, const void *rho);
+
 /* ---------------------------------------------------------------- discrete adjoint */
 
 /* Hand-written discrete adjoint of the spatial operator F(b) = DB (volume terms, Hall term

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <map>
 #include <memory>
 #include <set>
@@ -144,4 +145,16 @@ struct ieq_ctx {
   std::vector<std::string> *labels = nullptr;
   int gate_target = -1;
   int gate_count = 0;
+  // ieq_stages_*: the fused step enqueued stage by stage.  gate_target == -3 lets only the
+  // launches of stage gate_stage through (stage_count: the stage being enqueued); stage_trace
+  // receives the state buffers at the start of every stage (b1, b1', b2, b2', last input)
+  int gate_stage = -1, stage_count = 0;
+  std::vector<std::array<void *, 5>> *stage_trace = nullptr;
+  struct Stages {
+    bool active = false;
+    int integ = -1, conv = 1, count = 0, last = -1, saved_diss = 0;
+    std::array<void *, 5> step{};              // buffers at the start of the current step
+    std::vector<std::array<void *, 5>> trace;  // buffers at the start of every stage of a step
+    std::array<void *, 5> end{};               // buffers at the end of a step
+  } stages;
 };

@@ -11,9 +11,11 @@ reach ORDER/2.  The rank's context is the global settings with NODES_Z = (z1_k -
 the global spacing, the grid periodic, and the slab's z offset, so that testcase coordinates
 (init, u_analytical, analytical_b) are those of the global grid.
 
-A step runs the reference's kernel list of the integrator (compute_numerical_solution_setup.m
-:140-371) on the local slab.  After every kernel that writes a state field (every kernel but
-calc_curlB_rho_*, calc_u_* and calc_time_*), the state fields' ghost planes are refreshed from
+A step runs the integrator on the local slab either through the context's fused stage kernels,
+one RK stage at a time (ieq_stages_*: the ghost planes of the state fields are refreshed after
+every stage), or as the reference's kernel list (compute_numerical_solution_setup.m:140-371).
+After every stage -- every kernel of the list that writes a state field (all but
+calc_curlB_rho_*, calc_u_* and calc_time_*) -- the state fields' ghost planes are refreshed from
 the neighbours' owned planes: the G planes at the bottom of the owned range go to the rank
 below, the G at the top to the rank above, periodically (rank 0's lower neighbour is rank
 P-1) -- one point-to-point exchange per neighbour and field (NCCL between GPUs, gloo on CPU).
@@ -181,6 +183,14 @@ def ghost_depth(order: int) -> int:
 TWO_FIELD_INTEGRATORS = ("CarpenterKennedy2N54", "ToulorgeDesmet2N84F")
 
 
+class _DeviceArray:
+    """A 1-D device array by address (the CUDA array interface), for torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int, dtype):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dtype).str,
+                                         "data": (int(ptr), False), "version": 3}
+
+
 class SlabSolve:
     """One rank's slab of a decomposed periodic solve on its GPU: the local context (the C
     ABI's reference kernels, ieq_run_kernels) on torch device buffers, the ghost exchanges
@@ -232,13 +242,54 @@ class SlabSolve:
     def state(self):
         return [self.b, self.b2, self.b3] if self.nf == 3 else [self.b, self.b2]
 
-    def steps(self, num_steps: int) -> None:
-        decomposed_steps(self.slabs, self.ctx, self.seq, num_steps, self.state, self.args, self._sync)
+    def steps(self, num_steps: int, fused: bool = True) -> None:
+        """num_steps steps of the slab.  fused: the context's fused stage kernels, one RK stage
+        at a time (ieq_stages_*), the ghost planes of the state fields refreshed after every
+        stage; otherwise the reference kernel list with an exchange after every kernel that
+        writes the state."""
+        if not fused:
+            decomposed_steps(self.slabs, self.ctx, self.seq, num_steps, self.state, self.args, self._sync)
+            self._sync()
+            return
+        import torch
+        a = self.args
+        b3 = a[2] if self.nf == 3 else None
+        cb, u, rho, time = (a[3], a[4], a[5], a[6]) if self.nf == 3 else (a[2], a[3], a[4], a[5])
         self._sync()
+        ns = self.ctx.stages_begin(a[0], a[1], b3, cb, u)
+        try:
+            # the exchanges go on the context's stream, behind the stage that wrote the planes
+            # and ahead of the next one: no host synchronisation between stages
+            with torch.cuda.stream(torch.cuda.ExternalStream(self.ctx.stream, device=self.device)):
+                for _ in range(num_steps):
+                    for s in range(ns):
+                        self.ctx.stages_run(rho, time, s)
+                        self.slabs.exchange(*self._stage_planes())
+        finally:
+            self.ctx.stages_end(a[0], a[1], b3, cb, u, rho)
+        self._sync()
+
+    def _stage_planes(self):
+        """Zero-copy views of the component planes of the fused state fields (b1, b2[, b3]) as
+        they stand; the fused path moves a field between two buffers, so the views are cached
+        by buffer."""
+        import torch
+        cache = self.__dict__.setdefault("_views", {})
+        n = self.ctx.n_pad
+        size = np.dtype(self.ctx.real).itemsize
+        views = []
+        for f in range(self.nf):
+            base, stride = self.ctx.stages_field(f)
+            if base not in cache:
+                cache[base] = [torch.as_tensor(_DeviceArray(base + c * stride * size, n, self.ctx.real),
+                                               device=torch.device("cuda", self.device)) for c in range(3)]
+            views += cache[base]
+        return views
 
     def owned(self, field) -> np.ndarray:
         """The owned planes of a field as a host array (rows of the global planes z0..z1)."""
         return field[self.slabs.owned_rows()].cpu().numpy()
 
     def close(self) -> None:
+        self.__dict__.pop("_views", None)   # views of the context's memory
         self.ctx.close()

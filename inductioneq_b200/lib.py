@@ -88,6 +88,10 @@ def load() -> ctypes.CDLL:
     lib.ieq_check_finite.argtypes = [vp, vp]
     lib.ieq_test_brick_wait.argtypes = [vp, ctypes.c_int]
     lib.ieq_step_kernels.argtypes = [vp, ctypes.c_char_p, sz, ctypes.POINTER(ctypes.c_int)]
+    lib.ieq_stages_begin.argtypes = [vp] * 6 + [ctypes.POINTER(ctypes.c_int)]
+    lib.ieq_stages_run.argtypes = [vp, vp, vp, ctypes.c_int]
+    lib.ieq_stages_field.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_longlong)]
+    lib.ieq_stages_end.argtypes = [vp] * 7
     lib.ieq_profile_step.argtypes = [vp] * 8 + [ctypes.c_int, ctypes.c_int, ctypes.POINTER(KernelRecord),
                                                 ctypes.POINTER(ctypes.c_int)]
     lib.ieq_operator_jvp.argtypes = [vp] * 6
@@ -224,6 +228,28 @@ class Context:
         buf = ctypes.create_string_buffer(64 * max(n.value, 1))
         self._check(self.lib.ieq_step_kernels(self.h, buf, len(buf), ctypes.byref(n)))
         return [k for k in buf.value.decode().split("\n") if k]
+
+    # ---------------------------------------------------------------- stage by stage
+    def stages_begin(self, b, b2, b3, curlB_rho, u) -> int:
+        """Start stage-by-stage fused stepping (ieq_stages_begin); the stages of one step."""
+        n = ctypes.c_int(0)
+        self._check(self.lib.ieq_stages_begin(self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u),
+                                              ctypes.byref(n)))
+        return n.value
+
+    def stages_run(self, rho, time, stage: int) -> None:
+        self._check(self.lib.ieq_stages_run(self.h, _ptr(rho), _ptr(time), int(stage)))
+
+    def stages_field(self, field: int) -> tuple[int, int]:
+        """(device address of the x plane, component stride in elements) of state field
+        `field` (0 b1, 1 b2, 2 b3) after the last stage run."""
+        p, st = ctypes.c_void_p(), ctypes.c_longlong()
+        self._check(self.lib.ieq_stages_field(self.h, int(field), ctypes.byref(p), ctypes.byref(st)))
+        return p.value or 0, st.value
+
+    def stages_end(self, b, b2, b3, curlB_rho, u, rho) -> None:
+        self._check(self.lib.ieq_stages_end(self.h, _ptr(b), _ptr(b2), _ptr(b3), _ptr(curlB_rho), _ptr(u),
+                                            _ptr(rho)))
 
     def kernel(self, name: str, *args) -> None:
         """The typed entry point ieq_<name> (reference NDRange)."""

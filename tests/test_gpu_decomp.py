@@ -1,9 +1,10 @@
 """The z-slab decomposition on the GPU with one rank: the slab (the whole grid plus ghost
-planes refreshed by a local copy) runs the reference kernel lists through the C ABI on torch
-device buffers; its owned planes equal the undecomposed run of the same kernel lists bit for
-bit.  The variable-velocity case checks that the slab's testcase coordinates are the global
-grid's (IEQ_Z_OFFSET / IEQ_NZ_GLOBAL).  Several ranks are covered on CPU
-(tests/test_decomp_cpu.py); this run has one GPU."""
+planes refreshed by a local copy) runs the fused stage kernels one RK stage at a time
+(ieq_stages_*) or the reference kernel lists through the C ABI on torch device buffers; its
+owned planes equal the undecomposed run of the same kernels bit for bit.  The
+variable-velocity case checks that the slab's testcase coordinates are the global grid's
+(IEQ_Z_OFFSET / IEQ_NZ_GLOBAL).  Several ranks are covered on CPU (tests/test_decomp_cpu.py);
+this run has one GPU."""
 from __future__ import annotations
 
 import math
@@ -26,11 +27,15 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_single_slab_equals_undecomposed_kernel_lists(name):
+def test_single_slab_equals_undecomposed_run(name, fused):
+    # fused: the slab steps through the fused stage kernels one RK stage at a time
+    # (ieq_stages_*), the undecomposed grid through ieq_time_steps' fused path; else both run
+    # the reference kernel lists
     c = CASES[name]
     steps = 3
-    g = maps_for(dict(c, stage_kernel="LIST")).context()
+    g = maps_for(dict(c, stage_kernel="AUTO" if fused else "LIST")).context()
     b, u = g.vec(), g.vec()
     g.kernel("init_b", b)
     g.kernel("init_u", u)
@@ -43,7 +48,7 @@ def test_single_slab_equals_undecomposed_kernel_lists(name):
     t_ref = g.get_scalar(dev[6], n=2)
     s = SlabSolve(maps_for(c), R.Ranks(1, 0, 0))
     s.load(bh[: g.n], uh[: g.n], np.ones(g.n))
-    s.steps(steps)
+    s.steps(steps, fused=fused)
     np.testing.assert_array_equal(s.owned(s.b), ref[0])
     np.testing.assert_array_equal(s.owned(s.b2), ref[1])
     if s.nf == 3:
