@@ -56,3 +56,40 @@ def test_single_slab_equals_undecomposed_run(name, fused):
     np.testing.assert_array_equal(s.time.cpu().numpy(), t_ref)
     s.close()
     g.close()
+
+
+def test_stage_api_refuses_misuse():
+    # ieq_stages_*: a stage outside begin/end, an index out of range, a second begin, a LIST
+    # context; a full step through every stage equals ieq_time_steps
+    from inductioneq_b200.lib import IeqError
+    c = CASES["whistler_6c_hod_ck"]
+    ctx = maps_for(c).context()
+    b, b2, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+    rho, t = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+    ctx.kernel("init_b", b)
+    with pytest.raises(IeqError):
+        ctx.stages_run(rho, t, 0)
+    ns = ctx.stages_begin(b, b2, None, cb, u)
+    assert ns == 5                                  # CarpenterKennedy2N54
+    with pytest.raises(IeqError):
+        ctx.stages_begin(b, b2, None, cb, u)
+    for bad in (-1, ns):
+        with pytest.raises(IeqError):
+            ctx.stages_run(rho, t, bad)
+    for s in range(ns):
+        ctx.stages_run(rho, t, s)
+    ctx.stages_end(b, b2, None, cb, u, rho)
+    ref = maps_for(c).context()
+    rb, rb2, rcb, ru = ref.vec(), ref.vec(), ref.vec(), ref.vec()
+    rt = ref.scalar(np.zeros(2), n=2)
+    ref.kernel("init_b", rb)
+    ref.time_steps(rb, rb2, None, rcb, ru, ref.scalar(np.ones(ref.n_pad)), rt, 1)
+    np.testing.assert_array_equal(ctx.get_vec(b), ref.get_vec(rb))
+    np.testing.assert_array_equal(ctx.get_vec(b2), ref.get_vec(rb2))
+    np.testing.assert_array_equal(ctx.get_scalar(t, n=2), ref.get_scalar(rt, n=2))
+    ref.close()
+    ctx.close()
+    lst = maps_for(dict(c, stage_kernel="LIST")).context()
+    with pytest.raises(IeqError):
+        lst.stages_begin(lst.vec(), lst.vec(), None, lst.vec(), lst.vec())
+    lst.close()
