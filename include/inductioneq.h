@@ -271,11 +271,14 @@ ieq_status ieq_operator_vjp(ieq_ctx *ctx, const void *b, const void *w, const vo
  * -DIEQ_VARIABLE_U=1, else the given u) */
 ieq_status ieq_ssprk33_step_vjp(ieq_ctx *ctx, const void *s1, const void *s2, const void *s3, double t0,
                                 void *lambda, const void *u, const void *rho);
-/* Gradient through num_steps steps of the configured integrator -- SSPRK33 or one of the 2N
- * low-storage schemes CarpenterKennedy2N54 / ToulorgeDesmet2N84F -- from b0 at t = 0: lambda
- * holds dL/db(T) on entry and dL/db0 on return.  The forward run is checkpointed every
- * checkpoint_every steps and each segment recomputed (stage states kept) during the reverse
- * sweep; a 2N step is reversed stage by stage (mu2 += B_s mu1, mu1 += h F'^T mu2, mu2 = A_s mu2). */
+/* Gradient through num_steps steps of the configured integrator (any of the six) from b0 at
+ * t = 0: lambda holds dL/db(T) on entry and dL/db0 on return.  The forward run is checkpointed
+ * every checkpoint_every steps and each segment recomputed (the input of every stage kept)
+ * during the reverse sweep.  SSPRK33 and the 2N schemes have step adjoints of their own (a 2N
+ * step reversed stage by stage: mu2 += B_s mu1, mu1 += h F'^T mu2, mu2 = A_s mu2); the 2R
+ * schemes and SSPRK104 -- and every integrator with -DIEQ_ADJOINT_PROGRAM=1 -- reverse the
+ * step's register program (each stage K = h F(R_src) and its register updates, transposed in
+ * reverse order); that form needs the fused kernels (not -DIEQ_STAGE_KERNEL=LIST). */
 ieq_status ieq_adjoint_steps(ieq_ctx *ctx, const void *b0, void *lambda, const void *u, const void *rho,
                              int num_steps, int checkpoint_every);
 

@@ -710,6 +710,49 @@ ieq_status rk2n_step_vjp_ws(ieq_ctx *c, bool ck, void *const *x, double t0, void
   return IEQ_OK;
 }
 
+// lambda <- (d step / d b_n)^T lambda for one step given as a register program
+// (rk_step_program: every integrator) from the stage inputs x[e] of the e-th evaluating
+// stage of a step that started at t0.  Adjoint registers L0 = lambda, L1 = L2 = 0; the stages
+// in reverse order, each assignment R[dst] = sum a[r] R[r] + k K transposed newest first
+// (t = L[dst]; L[dst] = a[dst] t; L[r] += a[r] t for r != dst; LK += k t), then the stage's
+// evaluation K = h F(R[src]) transposed: L[src] += h F'(x)^T LK (the vjp's epilogue).
+// No allocation, no synchronisation
+ieq_status program_step_vjp_ws(ieq_ctx *c, const RkProgram &prog, void *const *x, double t0, void *lambda,
+                               const void *u, const void *rho, const VjpWork &w, void *L1, void *L2, void *LK,
+                               void *tmp) {
+  void *J0 = w.f[0], *gJr = w.f[1], *z = w.f[2], *uw = w.f[6];
+  void *L[3] = {lambda, L1, L2};
+  const size_t vb = c->n_pad * sizeof(R4<double>);
+  cudaMemsetAsync(L1, 0, vb, c->stream);
+  cudaMemsetAsync(L2, 0, vb, c->stream);
+  int e = prog.evaluations;
+  for (int si = (int)prog.stages.size() - 1; si >= 0; --si) {
+    const RkStage &st = prog.stages[si];
+    if (st.src >= 0) {
+      cudaMemsetAsync(LK, 0, vb, c->stream);
+      --e;
+    }
+    for (int ai = (int)st.as.size() - 1; ai >= 0; --ai) {
+      const RkAssign &as = st.as[ai];
+      lincomb(c, tmp, 1.0, L[as.dst], 0.0, nullptr);
+      lincomb(c, L[as.dst], as.a[as.dst], tmp, 0.0, nullptr);
+      for (int r = 0; r < 3; ++r)
+        if (r != as.dst && as.a[r] != 0.0) lincomb(c, L[r], 1.0, L[r], as.a[r], tmp);
+      if (st.src >= 0 && as.k != 0.0) lincomb(c, LK, 1.0, LK, as.k, tmp);
+    }
+    if (st.src >= 0) {
+      Epi ep;
+      ep.dst = L[st.src];
+      ep.x = L[st.src];
+      ep.al = 1.0;
+      ep.ga = st.h;
+      const ieq_status r = vjp(c, x[e], LK, stage_u(c, u, uw, w.d_time, t0 + st.t), rho, z, J0, gJr, ep);
+      if (r != IEQ_OK) return r;
+    }
+  }
+  return IEQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -801,9 +844,15 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   if (st != IEQ_OK) return st;
   const bool ssp = c->s.integrator == "SSPRK33";
   const bool ck2n = c->s.integrator == "CarpenterKennedy2N54", td2n = c->s.integrator == "ToulorgeDesmet2N84F";
-  if (!ssp && !ck2n && !td2n)
-    return afail(c, IEQ_ERR_SETTINGS,
-                 "the adjoint time stepping is SSPRK33, CarpenterKennedy2N54 or ToulorgeDesmet2N84F");
+  const int integ = integrator_id(c->s.integrator);
+  if (integ < 0) return afail(c, IEQ_ERR_SETTINGS, "no time integrator (-DIEQ_INTEGRATOR=...) in the settings");
+  // SSPRK33 and the 2N schemes have step adjoints of their own; the other integrators (and
+  // every one with IEQ_ADJOINT_PROGRAM=1) reverse the step's register program
+  const bool program = !(ssp || ck2n || td2n) || c->s.adjoint_program;
+  if (program && c->s.stage_kernel == 4)
+    return afail(c, IEQ_ERR_SETTINGS, "the register-program adjoint recomputes the forward with the fused kernels");
+  RkProgram prog;
+  if (program) rk_step_program(integ, c->s.dt, prog);
   cudaSetDevice(c->device);
   const size_t vb = c->n_pad * sizeof(R4<double>);
   const int K = checkpoint_every;
@@ -811,15 +860,17 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
   // states kept per step: SSPRK33 its three stage states, a 2N scheme the input of every stage
   const double *A2, *B2, *C2;
   int S2 = 0;
-  if (!ssp) rk2n_coefficients(ck2n, &A2, &B2, &C2, &S2);
-  const int P = ssp ? 3 : S2;
-  // checkpoints (nseg), the stage states of one segment (P K), step work (5), step-adjoint work (7)
+  if (ck2n || td2n) rk2n_coefficients(ck2n, &A2, &B2, &C2, &S2);
+  const int P = program ? prog.evaluations : ssp ? 3 : S2;
+  // checkpoints (nseg), the stage states of one segment (P K), step work (5), step-adjoint
+  // work (7), the program's adjoint registers L1, L2, LK and a temporary (4)
   std::vector<void *> pool;
-  if ((st = adj_pool(c, (size_t)nseg + (size_t)P * K + 12, vb, pool)) != IEQ_OK) return st;
+  if ((st = adj_pool(c, (size_t)nseg + (size_t)P * K + 16, vb, pool)) != IEQ_OK) return st;
   std::vector<void *> ck(pool.begin(), pool.begin() + nseg), seg(pool.begin() + nseg, pool.begin() + nseg + P * K),
       w(pool.begin() + nseg + P * K, pool.begin() + nseg + P * K + 5);
   VjpWork vw;
-  vw.f.assign(pool.begin() + nseg + P * K + 5, pool.end());
+  vw.f.assign(pool.begin() + nseg + P * K + 5, pool.begin() + nseg + P * K + 12);
+  void *const *preg = &pool[(size_t)nseg + (size_t)P * K + 12];   // L1, L2, LK, tmp
   vw.d_time = c->adj_time + 2;
   void *cur = w[0], *b2 = w[1], *b3 = w[2], *cb = w[3], *uw = w[4];
   double *d_time = c->adj_time;
@@ -890,8 +941,11 @@ ieq_status ieq_adjoint_steps(ieq_ctx *c, const void *b0, void *lambda, const voi
     st = advance(cur, t0s[n0], n1 - n0, seg.data());
     for (int n = n1 - 1; n >= n0 && st == IEQ_OK; --n) {
       void *const *x = &seg[(size_t)P * (n - n0)];
-      st = ssp ? ssprk33_step_vjp_ws(c, x[0], x[1], x[2], t0s[n], lambda, u, rho, vw)
-               : rk2n_step_vjp_ws(c, ck2n, x, t0s[n], lambda, u, rho, vw);
+      if (program)
+        st = program_step_vjp_ws(c, prog, x, t0s[n], lambda, u, rho, vw, preg[0], preg[1], preg[2], preg[3]);
+      else
+        st = ssp ? ssprk33_step_vjp_ws(c, x[0], x[1], x[2], t0s[n], lambda, u, rho, vw)
+                 : rk2n_step_vjp_ws(c, ck2n, x, t0s[n], lambda, u, rho, vw);
     }
   }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == IEQ_OK) st = afail(c, IEQ_ERR_CUDA, "adjoint sweep");

@@ -72,6 +72,9 @@ struct Settings {
   // IEQ_HODP: Hall + high-order dissipation -- 1 the curl kernel forms the dissipation sum and
   // the stage kernel reads it; 0 the stage kernel gathers the dissipation rows itself
   int hodp = 1;
+  // IEQ_ADJOINT_PROGRAM: 1 reverses SSPRK33 and the 2N schemes through the generic register
+  // program of the step as well (the other integrators always use it)
+  int adjoint_program = 0;
   // IEQ_CURL_Z: the curl kernel of periodic Hall stages as the 2.5D z march (stage_z.cuh):
   // 0 never, 1 always, 2 (default) on grids of at least kCurlZAutoNodes nodes
   int curl_z = 2;
@@ -94,6 +97,27 @@ struct SbpOperator {
   bool has_lap[3] = {false, false, false};
 };
 bool load_operator(int order, bool extended, SbpOperator &op, std::string &err);
+
+// One step of a time integrator as a register program (R0 = b1, the solution; R1 = b2;
+// R2 = b3 or db): stage s evaluates K = h F(R[src]) at time t0 + t (src < 0: no evaluation),
+// then runs its assignments R[dst] = a[0] R0 + a[1] R1 + a[2] R2 + k K in order.  Built from
+// the coefficient tables of the fused time step (rk_step_program); the discrete adjoint
+// reverses it.
+struct RkAssign {
+  int dst;
+  double a[3];
+  double k;
+};
+struct RkStage {
+  int src;
+  double h, t;
+  std::vector<RkAssign> as;
+};
+struct RkProgram {
+  std::vector<RkStage> stages;
+  int evaluations = 0;   // stages with src >= 0 (the stage inputs the adjoint keeps)
+};
+void rk_step_program(int integ, double dt, RkProgram &p);
 
 }  // namespace ieq
 

@@ -170,6 +170,12 @@ bool parse_settings(const char *settings, const char *const *paths, int n_paths,
         return false;
       }
       s.curl_z = std::atoi(val.c_str());
+    } else if (key == "IEQ_ADJOINT_PROGRAM") {
+      if (val != "0" && val != "1") {
+        err = "IEQ_ADJOINT_PROGRAM must be 0 or 1";
+        return false;
+      }
+      s.adjoint_program = std::atoi(val.c_str());
     } else if (key == "IEQ_HODP") {
       if (val != "0" && val != "1") {
         err = "IEQ_HODP must be 0 or 1";

@@ -128,6 +128,8 @@ class Maps:
             s += f" -DIEQ_HODP={int(self.I_Tech['hodp'])}"
         if self.I_Tech.get("cg_pass_a") is not None:   # the CG's pass A: 2 the 2.5D kernel, 1 per-node gathers
             s += f" -DIEQ_CG_PASS_A={int(self.I_Tech['cg_pass_a'])}"
+        if self.I_Tech.get("adjoint_program") is not None:   # 1: the register-program step adjoint for every integrator
+            s += f" -DIEQ_ADJOINT_PROGRAM={int(self.I_Tech['adjoint_program'])}"
         if self.I_Tech.get("nz_global"):   # a z slab of a decomposed grid (inductioneq_b200.decomp)
             s += f" -DIEQ_Z_OFFSET={int(self.I_Tech['z_offset'])} -DIEQ_NZ_GLOBAL={int(self.I_Tech['nz_global'])}"
         return s

@@ -38,6 +38,7 @@ def maps_for(c: dict) -> Maps:
     m.I_Tech["cg_pass_a"] = c.get("cg_pass_a")
     m.I_Tech["curl_z"] = c.get("curl_z")
     m.I_Tech["hodp"] = c.get("hodp")
+    m.I_Tech["adjoint_program"] = c.get("adjoint_program")
     m.I_RunOps.update({"order": c.get("order", 4), "operator_form": "extended" if c.get("extended") else "classical",
                        "testcase": c["testcase"], "variable_u": c.get("variable_u", False),
                        "periodic": "USE_PERIODIC" if c.get("periodic") else "NONE"})

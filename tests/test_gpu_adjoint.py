@@ -6,8 +6,9 @@
 * the checkpointed SSPRK33 gradient of a final-time L2 misfit against central differences
   along seeded random directions (Richardson-extrapolated, relative 1e-6), driven through a torch.autograd.Function
   (defined here, in the test harness only);
-* the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F), and for
-  Hall on boxes (the outflow SAT) and first-order dissipation.
+* the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F), for the
+  2R schemes and SSPRK104 (the step's register program reversed), and for Hall on boxes (the
+  outflow SAT) and first-order dissipation.
 """
 from __future__ import annotations
 
@@ -349,8 +350,10 @@ def test_adjoint_of_adaptive_dissipation_is_refused():
     ctx.close()
 
 
-def test_adjoint_of_an_unsupported_integrator_is_refused():
-    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16), integrator="KennedyCarpenterLewis2R54C")
+def test_program_adjoint_of_a_list_run_is_refused():
+    # the register-program adjoint (2R schemes, SSPRK104) recomputes the forward with the
+    # fused kernels: IEQ_STAGE_KERNEL=LIST is refused
+    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16), integrator="KennedyCarpenterLewis2R54C", stage_kernel="LIST")
     ctx = maps_for(dict(c, dt=1e-3)).context()
     b, u = ctx.vec(), ctx.vec()
     lam = ctx.vec()
@@ -358,6 +361,84 @@ def test_adjoint_of_an_unsupported_integrator_is_refused():
     with pytest.raises(IeqError) as e:
         ctx.adjoint_steps(b, lam, u, ctx.scalar(np.ones(ctx.n_pad)), 2, 1)
     assert e.value.name == "IEQ_ERR_SETTINGS"
+    ctx.close()
+
+
+def _hallper16(integrator, **kw):
+    c = dict(CASES["hallper_4c"], nodes=(16, 16, 16), integrator=integrator, **kw)
+    probe = maps_for(dict(c, dt=1.0)).context()
+    u = probe.vec()
+    probe.kernel("init_u", u)
+    umax = float(np.sqrt((probe.get_vec(u)[:, :3] ** 2).sum(1)).max())
+    probe.close()
+    return c, (2.0 / 16) * (HP / 16) / umax        # CFL 2/N (compute_error_hall_periodic.m:51)
+
+
+@pytest.mark.parametrize("integrator", ["SSPRK33", "CarpenterKennedy2N54", "ToulorgeDesmet2N84F"])
+def test_register_program_adjoint_equals_the_dedicated_step_adjoints(integrator):
+    # IEQ_ADJOINT_PROGRAM=1 reverses SSPRK33 and the 2N schemes through the generic register
+    # program as well: the same gradient as their dedicated step adjoints (the pointwise
+    # combinations in another order: 1e-13 of its scale)
+    c, dt = _hallper16(integrator)
+    out = []
+    for prog in (0, 1):
+        ctx = maps_for(dict(c, dt=dt, adjoint_program=prog)).context()
+        b, u = ctx.vec(), ctx.vec()
+        ctx.kernel("init_b", b)
+        ctx.kernel("init_u", u)
+        lam = ctx.vec(_rand(ctx, 9))
+        ctx.adjoint_steps(b, lam, u, ctx.scalar(np.ones(ctx.n_pad)), 7, 3)
+        out.append(ctx.get_vec(lam)[:, :3])
+        ctx.close()
+    assert np.abs(out[0] - out[1]).max() <= 1e-13 * np.abs(out[0]).max()
+
+
+@pytest.mark.parametrize("integrator", ["KennedyCarpenterLewis2R54C", "CalvoFrancoRandez2R64", "SSPRK104"])
+def test_register_program_adjoint_matches_central_differences(integrator):
+    # the 2R schemes and SSPRK104 through the register-program adjoint: the checkpointed
+    # gradient against Richardson-extrapolated central differences of the time stepping
+    c, dt = _hallper16(integrator)
+    ctx = maps_for(dict(c, dt=dt)).context()
+    nsteps, every = 7, 3
+    b = ctx.vec()
+    ctx.kernel("init_b", b)
+    rho = ctx.scalar(np.ones(ctx.n_pad))
+    b0 = ctx.get_vec(b)
+    n = ctx.n
+
+    def forward(x):
+        bb, b2, b3, cb, uu = ctx.vec(x), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+        ctx.kernel("init_u", uu)
+        ctx.time_steps(bb, b2, b3, cb, uu, rho, ctx.scalar(np.zeros(2), n=2), nsteps)
+        return ctx.get_vec(bb)
+
+    rng = np.random.default_rng(29)
+    target = forward(b0) + 1e-3 * rng.standard_normal((ctx.n_pad, 4))
+    target[:, 3] = 0
+    target[n:] = 0
+
+    def loss(x):
+        d = forward(x)[:n, :3] - target[:n, :3]
+        return 0.5 * float(np.sum(d * d))
+
+    g0 = np.zeros_like(b0)
+    g0[:n, :3] = forward(b0)[:n, :3] - target[:n, :3]
+    lam = ctx.vec(g0)
+    uu = ctx.vec()
+    ctx.kernel("init_u", uu)
+    ctx.adjoint_steps(ctx.vec(b0), lam, uu, rho, nsteps, every)
+    grad = ctx.get_vec(lam)
+    for k in range(3):
+        d = rng.standard_normal((ctx.n_pad, 4))
+        d[:, 3] = 0
+        d[n:] = 0
+        d /= np.sqrt(np.sum(d[:, :3] ** 2))
+        ad = float(np.sum(grad[:, :3] * d[:, :3]))
+
+        def cd(e):
+            return (loss(b0 + e * d) - loss(b0 - e * d)) / (2 * e)
+        rich = (4.0 * cd(5e-4) - cd(1e-3)) / 3.0
+        assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
     ctx.close()
 
 
