@@ -61,6 +61,11 @@ BASE = " -DNODES_X=16 -DNODES_Y=16 -DNODES_Z=16 -DXMIN=0 -DXMAX=1 -DYMIN=0 -DYMA
     (BASE + " -DIEQ_PDL=2", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_PDL"),
     (BASE + " -DIEQ_STAGE_KERNEL=FAST", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "ZMARCH"),
     (BASE + " -DIEQ_ZMARCH_TZ=-1", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_ZMARCH_TZ"),
+    (BASE + " -DIEQ_HODP=2", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_HODP"),
+    (BASE + " -DIEQ_CURL_Z=3", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_CURL_Z"),
+    (BASE + " -DIEQ_CG_PASS_A=3", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1, "IEQ_CG_PASS_A"),
+    (BASE + " -DIEQ_ADJOINT_PROGRAM=2", ["../include/4thOrder.h", "../include/rotation_3D.h"], 1,
+     "IEQ_ADJOINT_PROGRAM"),
 ])
 def test_bad_settings_are_rejected_on_the_host(settings, paths, status, msg):
     st, err = _create(settings, paths)
@@ -95,10 +100,11 @@ def test_kernel_selection_settings_are_emitted_and_accepted():
     m.I_TI["DT"] = 0.01
     m.I_RunOps["testcase"] = "rotation_3D"
     m.I_Tech.update({"stage_kernel": "ZMARCH", "col_block": (16, 4, 2), "curl_block": (8, 8, 2), "col_pairs": 4,
-                     "xband": 2, "pdl": 0, "zmarch_tz": 24})
+                     "xband": 2, "pdl": 0, "zmarch_tz": 24, "adjoint_program": 1, "hodp": 0})
     s = m.settings()
     for key in (" -DIEQ_STAGE_KERNEL=ZMARCH", " -DIEQ_COL_BLOCK=16x4x2", " -DIEQ_CURL_BLOCK=8x8x2",
-                " -DIEQ_COL_PAIRS=4", " -DIEQ_XBAND=2", " -DIEQ_PDL=0", " -DIEQ_ZMARCH_TZ=24"):
+                " -DIEQ_COL_PAIRS=4", " -DIEQ_XBAND=2", " -DIEQ_PDL=0", " -DIEQ_ZMARCH_TZ=24",
+                " -DIEQ_ADJOINT_PROGRAM=1", " -DIEQ_HODP=0"):
         assert key in s, key
     st, err = _create(s, m.kernel_path_list())
     assert st not in (1, 2), (st, err)    # neither a settings nor a shape error
