@@ -232,6 +232,64 @@ def form_fp32(dev, b_ref64):
             "note": "same workload, FP32 state and stencils"}
 
 
+def form_fp32_testcases(dev, n=48, steps=30):
+    """The precision form per testcase: every testcase of the reference (include/*.h) and the
+    two of this project on an n^3 grid, run in FP64 and in FP32 (state and stencils) from
+    their own initial fields: the mass-weighted L2 error against the exact field at the final
+    time (kernel_operator.cl:11-47 norm2_diff) in each precision, and the mass-weighted L2
+    difference of the FP32 field from the FP64 one (absolute and relative to ||B_64||)."""
+    import numpy as np
+
+    from inductioneq_b200.induction_eq import Maps
+    hp, tp = 4.0 * math.pi / 3.0, 2.0 * math.pi
+    cases = {   # testcase: (lo, hi, periodic, order, hall, variable u, dissipation, integrator, dt)
+        "rotation_2D": (-1.0, 1.0, False, 4, False, False, None, "SSPRK33", 0.5 * (2.0 / (n - 1)) / math.sqrt(2)),
+        "rotation_3D": (-1.0, 1.0, False, 4, False, False, None, "SSPRK33", 0.4 * (2.0 / (n - 1)) / 1.7),
+        "rotation_gaussian": (-1.0, 1.0, False, 4, False, False, None, "SSPRK33",
+                              0.5 * (2.0 / (n - 1)) / math.sqrt(2)),
+        "hall_periodic": (0.0, hp, True, 4, True, True, None, "CarpenterKennedy2N54", (2.0 / n) * (hp / n) / 2.0),
+        "hall_travelling_wave": (0.0, tp, False, 4, True, True, None, "SSPRK33", 1e-3),
+        "confined_domain": (0.0, 1.0, False, 4, True, False, None, "CarpenterKennedy2N54", 0.2 / (n - 1) ** 2),
+        "alfven_periodic_2D": (0.0, 1.0, True, 4, False, True, None, "CarpenterKennedy2N54", 0.2 / n),
+        "hall_circular_wave": (0.0, tp, True, 6, True, False, "USE_HIGH_ORDER_DISSIPATION", "CarpenterKennedy2N54",
+                               0.2 * (tp / n) ** 2),
+    }
+    out = {}
+    for tc, (lo, hi, per, order, hall, varu, diss, integ, dt) in cases.items():
+        fields, res = {}, {}
+        for real in ("double", "float"):
+            m = Maps()
+            m.I_Mesh.update({"NODES_X": n, "NODES_Y": n, "NODES_Z": n, "XMIN": lo, "XMAX": hi, "YMIN": lo,
+                             "YMAX": hi, "ZMIN": lo, "ZMAX": hi})
+            m.I_TI.update({"DT": dt, "time_integrator": integ})
+            if hall:
+                m.I_IEq["hall_term"] = "USE_HALL"
+            if diss:
+                m.I_IEq.update({"dissipation": "USE_ARTIFICIAL_DISSIPATION", "dissipation_form": diss})
+            m.I_RunOps.update({"order": order, "testcase": tc, "periodic": "USE_PERIODIC" if per else "NONE",
+                               "variable_u": varu})
+            m.I_Tech["REAL"] = real
+            ctx = m.context(device=dev)
+            b, b2, b3, cb, u = ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec()
+            rho, t = ctx.scalar(np.ones(ctx.n_pad)), ctx.scalar(np.zeros(2), n=2)
+            ctx.kernel("init_b", b)
+            ctx.kernel("init_u", u)
+            ctx.time_steps(b, b2, b3, cb, u, rho, t, steps)
+            res[real] = ctx.results(b, steps * dt, ctx.vec(), ctx.scalar())
+            fields[real] = ctx.get_vec(b).astype(np.float64)
+            if real == "double":
+                keep = ctx   # the FP64 context measures the difference below
+            else:
+                ctx.close()
+        d = math.sqrt(keep.norm2_diff(keep.vec(fields["float"]), keep.vec(fields["double"])))
+        nb = math.sqrt(keep.norm2(keep.vec(fields["double"])))
+        keep.close()
+        out[tc] = {"grid": [n] * 3, "steps": steps, "dt": dt, "integrator": integ, "order": order,
+                   "l2_err_vs_exact": {"fp64": res["double"]["abs_err"], "fp32": res["float"]["abs_err"]},
+                   "l2_diff_fp32_vs_fp64": {"abs": d, "rel": d / nb if nb > 0 else None}}
+    return out
+
+
 def form_batched(dev, steps=200):
     """32 rotation solves, N ~ U{16..96}, omega ~ U(0.5,2), order in {2,4,6}, 200 SSPRK33 steps,
     one persistent launch captured in a CUDA graph, tile shapes from the autotuner; also the
@@ -691,7 +749,8 @@ def main() -> None:
     ap.add_argument("--decomposed", action="store_true",
                     help="one 128^3 whistler solve decomposed into z slabs over the ranks")
     ap.add_argument("--form", default=None,
-                    help="run only this form (fp32, rotation_c1, hbm_256, batched, precision_c3, adjoint_c5) "
+                    help="run only this form (fp32, rotation_c1, hbm_256, batched, precision_c3, adjoint_c5, "
+                         "fp32_testcases) "
                          "on one GPU and print its JSON")
     a = ap.parse_args()
     from inductioneq_b200 import ranks as R
@@ -727,7 +786,7 @@ def main() -> None:
     torch.cuda.set_device(dev)
     if a.form:
         forms = {"rotation_c1": form_rotation40, "hbm_256": form_hbm256, "batched": form_batched,
-                 "precision_c3": form_precision, "adjoint_c5": form_adjoint}
+                 "precision_c3": form_precision, "adjoint_c5": form_adjoint, "fp32_testcases": form_fp32_testcases}
         print(json.dumps({a.form: forms[a.form](dev)}))
         R.finish(rk)
         return
@@ -924,7 +983,8 @@ def main() -> None:
         except Exception as e:   # a form that fails is reported, not fatal to the line
             out["forms"] = {"fp32": {"error": repr(e)}}
         for name, fn in (("rotation_c1", form_rotation40), ("hbm_256", form_hbm256), ("batched", form_batched),
-                         ("precision_c3", form_precision), ("adjoint_c5", form_adjoint)):
+                         ("precision_c3", form_precision), ("adjoint_c5", form_adjoint),
+                         ("fp32_testcases", form_fp32_testcases)):
             try:
                 out["forms"][name] = fn(dev)
             except Exception as e:
