@@ -30,8 +30,18 @@ constexpr int kMaxPartials = 65536;  // least size of the block-partial buffers 
 // leaves about 23 KB of L1, the B stencil loads hit L1 33 % of the time and the kernel is
 // L2-latency bound.  AUTO therefore never takes it; IEQ_STAGE_KERNEL=ZMARCH does.
 constexpr long long kZmarchAutoNodes = 1LL << 62;
-// grids from which IEQ_CURL_Z=2 (the default) runs the 2.5D curl kernel on periodic grids
-constexpr long long kCurlZAutoNodes = 1LL << 62;
+// IEQ_CURL_Z=2 (the default) runs the 2.5D curl kernel on periodic FP64 grids of more than
+// kCurlZAutoNodes nodes, with the dissipation sum and stencil radius 1 or 3.  Measured on B200
+// (whistler, CK2N54, step time against the pair curl kernel): 6th order + HOD 160^3 / 192^3 /
+// 256^3 +8.5 / +3.5 / +3.2 %, 128^3 -0.9 %; 2nd order + HOD +9 / +2 / +1 %; slower for 4th
+// order (-2..-4 % at 192^3 and 256^3), without the dissipation sum (-3 %) and in FP32 (the
+// four-node kernels, -6..-14 %).
+constexpr long long kCurlZAutoNodes = 1LL << 21;
+template <typename R>
+inline bool curl_z_auto(const ieq_ctx *c, bool hod) {
+  const int ri = c->op.order / 2;
+  return sizeof(R) == 8 && hod && (ri == 1 || ri == 3) && (long long)c->n > kCurlZAutoNodes;
+}
 
 #define IEQ_CUDA(ctx, call)                                                                    \
   do {                                                                                         \
@@ -296,11 +306,11 @@ void launch_curl_e_any(ieq_ctx *c, SoA<R> b, const R *rho, SoA<R> E, SoA<R> jfac
   }
   const bool per = c->s.periodic;
   // the 2.5D curl kernel (stage_z.cuh) on periodic grids: forced by IEQ_CURL_Z=1, or
-  // (IEQ_CURL_Z=2, the default) from kCurlZAutoNodes nodes on
-  if (per && (c->s.curl_z == 1 || (c->s.curl_z == 2 && (long long)c->n >= kCurlZAutoNodes))) {
+  // (IEQ_CURL_Z=2, the default) where curl_z_auto measured it faster
+  if (per && (c->s.curl_z == 1 || (c->s.curl_z == 2 && curl_z_auto<R>(c, hod)))) {
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    const int tz = cz_chunk(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2], nsm > 0 ? nsm : 148, 4);
+    const int tz = cz_chunk(c->s.nodes[0], c->s.nodes[1], c->s.nodes[2], nsm > 0 ? nsm : 148, 2 * kCzBlocks);
     switch (c->op_id) {
       case 0: launch_curl_e_z<R, 0>(a, hod, tz, c->s.pdl, c->stream); break;
       case 1: launch_curl_e_z<R, 1>(a, hod, tz, c->s.pdl, c->stream); break;

@@ -76,7 +76,7 @@ struct Settings {
   // program of the step as well (the other integrators always use it)
   int adjoint_program = 0;
   // IEQ_CURL_Z: the curl kernel of periodic Hall stages as the 2.5D z march (stage_z.cuh):
-  // 0 never, 1 always, 2 (default) on grids of at least kCurlZAutoNodes nodes
+  // 0 never, 1 always, 2 (default) where measured faster (api.cu: curl_z_auto)
   int curl_z = 2;
 };
 

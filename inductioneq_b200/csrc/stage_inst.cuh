@@ -416,11 +416,36 @@ void launch_curl_e_diag<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, con
   }
 }
 
+// one launch of k_curl_e_z<R, OP, H>; its ring is dynamic shared memory beside the static
+// plane buffers, allowed once per device for each instantiation
+template <typename R, int OP, bool H>
+void launch_cz(const CurlArgs<R, SoA<R>> &a, dim3 g, int tz, bool pdl, cudaStream_t s) {
+  constexpr int dyn = cz_ring_bytes<R>();
+  static bool ring_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !ring_set[dev]) {
+    cudaFuncSetAttribute(k_curl_e_z<R, OP, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (dev >= 0 && dev < 64) ring_set[dev] = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = dim3(kCzTX * kCzTY);
+  cfg.dynamicSmemBytes = dyn;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_curl_e_z<R, OP, H>, a, tz);
+}
+
 template <>
 void launch_curl_e_z<IEQ_R, IEQ_OP>(const CurlArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, int tz, bool pdl, cudaStream_t s) {
   const dim3 g((a.m.nx + kCzTX - 1) / kCzTX, (a.m.ny + kCzTY - 1) / kCzTY, (a.m.nz + tz - 1) / tz);
-  if (hod) launch_pdl(k_curl_e_z<IEQ_R, IEQ_OP, true>, g, dim3(kCzTX * kCzTY), s, pdl, a, tz);
-  else launch_pdl(k_curl_e_z<IEQ_R, IEQ_OP, false>, g, dim3(kCzTX * kCzTY), s, pdl, a, tz);
+  if (hod) launch_cz<IEQ_R, IEQ_OP, true>(a, g, tz, pdl, s);
+  else launch_cz<IEQ_R, IEQ_OP, false>(a, g, tz, pdl, s);
 }
 
 }  // namespace ieq

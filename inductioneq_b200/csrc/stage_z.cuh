@@ -385,44 +385,73 @@ namespace ieq {
 // loaded from global memory about once.  A CTA of kCzTX x kCzTY threads owns a tile of x-y
 // columns and a chunk of z planes; every thread keeps the three components of B of its
 // column at planes z - RI .. z + RI in registers (the z terms) and plane z of the tile with
-// its x and y halos (RI deep) sits in shared memory (the x and y terms).  The sums run in the
-// order of k_curl_e_hod (axis by axis, offsets ascending), so the outputs equal the one-node
-// kernels' up to the compiler's fused multiply-adds.
-constexpr int kCzTX = 32, kCzTY = 8;
+// its x and y halos (RI deep) sits in shared memory (the x and y terms).  The march is
+// software-pipelined: the column's queue values (B at plane z + RI, the only loads that
+// come from DRAM rather than from a neighbour's recent loads in L2) are copied kCzAhead
+// planes ahead into a per-thread shared-memory ring by cp.async (each thread reads back only
+// what it copied, so the ring needs no barrier), while the next plane's halo points and rho
+// are loaded into registers during the current plane's compute; the halo'd plane is
+// double-buffered in shared memory, so one barrier per plane suffices (a thread writes
+// buffer (z + 1) & 1 only after every thread passed the barrier of plane z, i.e. finished
+// plane z - 1, the last reader of that buffer).  The sums run in the order of k_curl_e_hod
+// (axis by axis, offsets ascending), so the outputs equal the one-node kernels' up to the
+// compiler's fused multiply-adds.  Registers are capped for kCzBlocks resident CTAs per SM
+// (80 in FP64, no spills; 2 CTAs of 120 registers measured 7 % slower at 256^3).
+constexpr int kCzTX = 32, kCzTY = 8, kCzBlocks = 3;
+constexpr int kCzAhead = 3;   // planes of the column's B loads in flight ahead of the march
+// ring slots: one more than the look-ahead, so that the slot refilled at plane z was last
+// read at plane z - 1, before the barrier of plane z
+constexpr int kCzSlots = kCzAhead + 1;
+// dynamic shared memory of k_curl_e_z: the ring of the column's B, kCzSlots x 3 x threads
+template <typename R>
+constexpr int cz_ring_bytes() { return kCzSlots * 3 * kCzTX * kCzTY * (int)sizeof(R); }
+
+// per-thread asynchronous copies (cp.async, L1-allocating) of one element into shared memory
+template <typename R>
+__device__ __forceinline__ void cz_async(R *dst, const R *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(R) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cz_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cz_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <typename R, int OP, bool HODS>
-__global__ void __launch_bounds__(kCzTX * kCzTY) k_curl_e_z(const __grid_constant__ CurlArgs<R, SoA<R>> a, int tz) {
+__global__ void __launch_bounds__(kCzTX * kCzTY, kCzBlocks)
+    k_curl_e_z(const __grid_constant__ CurlArgs<R, SoA<R>> a, int tz) {
   constexpr int RI = Op<OP>::RI, W = 2 * RI + 1;
   constexpr int SX = kCzTX + 2 * RI, SY = kCzTY + 2 * RI;
-  __shared__ R pl[3][SY][SX];
+  constexpr int NT = kCzTX * kCzTY;
+  constexpr int NHALO = 2 * RI * (kCzTX + kCzTY);   // x halos of the tile rows, y halos of its columns
+  constexpr int HPT = (NHALO + NT - 1) / NT;         // halo points per thread
+  __shared__ R pl[2][3][SY][SX];
+  extern __shared__ __align__(16) unsigned char cz_dyn[];
+  R(*qr)[3][NT] = reinterpret_cast<R(*)[3][NT]>(cz_dyn);   // ring of the column's B at plane z + RI
   pdl_enter();
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
   const int tx = threadIdx.x % kCzTX, ty = threadIdx.x / kCzTX;
   const int x0 = blockIdx.x * kCzTX, y0 = blockIdx.y * kCzTY;
   const int zb = blockIdx.z * tz, ze = min(zb + tz, nz);
   const int ix = x0 + tx, iy = y0 + ty;
+  const bool own = ix < nx && iy < ny;
   const long long sz = (long long)nx * ny;
   const long long cs = a.b.s;
+  const R *bp = a.b.p;
   auto wrap = [](int i, int n) { i %= n; return i < 0 ? i + n : i; };
   // the column of (ix, iy) wrapped into the grid (threads past the edge hold the periodic image)
   const long long col = wrap(ix, nx) + (long long)nx * wrap(iy, ny);
-  R q[3][W];
+  // this thread's halo points: offset within a shared component plane and grid column
+  int hpos[HPT];
+  long long hcol[HPT];
 #pragma unroll
-  for (int k = 0; k < W - 1; ++k) {
-    const long long j = col + sz * wrap(zb - RI + k, nz);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) q[c][k + 1] = __ldg(a.b.p + j + c * cs);
-  }
-  for (int z = zb; z < ze; ++z) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-#pragma unroll
-      for (int k = 0; k < W - 1; ++k) q[c][k] = q[c][k + 1];
-      q[c][W - 1] = __ldg(a.b.p + col + sz * wrap(z + RI, nz) + c * cs);
-      pl[c][ty + RI][tx + RI] = q[c][RI];
-    }
-    // halos of plane z: RI columns left and right of every tile row, RI rows above and below
-    for (int h = threadIdx.x; h < 2 * RI * kCzTY + 2 * RI * kCzTX; h += kCzTX * kCzTY) {
+  for (int k = 0; k < HPT; ++k) {
+    const int h = threadIdx.x + k * NT;
+    hpos[k] = -1;
+    hcol[k] = 0;
+    if (h < NHALO) {
       int px, py;
       if (h < 2 * RI * kCzTY) {
         const int side = h / (RI * kCzTY), rem = h % (RI * kCzTY);
@@ -434,12 +463,67 @@ __global__ void __launch_bounds__(kCzTX * kCzTY) k_curl_e_z(const __grid_constan
         px = RI + rem % kCzTX;
         py = side ? kCzTY + RI + rem / kCzTX : rem / kCzTX;
       }
-      const long long j = wrap(x0 - RI + px, nx) + (long long)nx * wrap(y0 - RI + py, ny) + sz * z;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) pl[c][py][px] = __ldg(a.b.p + j + c * cs);
+      hpos[k] = py * SX + px;
+      hcol[k] = wrap(x0 - RI + px, nx) + (long long)nx * wrap(y0 - RI + py, ny);
     }
+  }
+  R q[3][W];
+#pragma unroll
+  for (int k = 0; k < W - 1; ++k) {
+    const long long j = col + sz * wrap(zb - RI + k, nz);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) q[c][k + 1] = __ldg(bp + j + c * cs);
+  }
+  // the column's B at plane z + RI into ring slot (z - zb) % kCzSlots, one commit group per
+  // plane (empty past the chunk, so that every plane waits for the same group count)
+  auto issue = [&](int z) {
+    if (z < ze) {
+      int zq = z + RI;
+      if (zq >= nz) zq -= nz;
+      const long long jq = col + sz * zq;
+      const int slot = (z - zb) % kCzSlots;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cz_async(&qr[slot][c][threadIdx.x], bp + jq + c * cs);
+    }
+    cz_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < kCzAhead; ++k) issue(zb + k);
+  // registers of the next plane: halo points, rho
+  R nh[HPT][3], nr = (R)1;
+  auto fetch = [&](int z) {
+    const long long zo = sz * z;
+#pragma unroll
+    for (int k = 0; k < HPT; ++k)
+      if (hpos[k] >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nh[k][c] = __ldg(bp + hcol[k] + zo + c * cs);
+      }
+    if (a.rho && own) nr = __ldg(a.rho + ix + (long long)nx * iy + zo);
+  };
+  fetch(zb);
+  for (int z = zb; z < ze; ++z) {
+    R(*P)[SY][SX] = pl[(z - zb) & 1];
+    cz_wait<kCzAhead - 1>();
+    const int slot = (z - zb) % kCzSlots;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) q[c][k] = q[c][k + 1];
+      q[c][W - 1] = qr[slot][c][threadIdx.x];
+      P[c][ty + RI][tx + RI] = q[c][RI];
+    }
+#pragma unroll
+    for (int k = 0; k < HPT; ++k)
+      if (hpos[k] >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) (&P[c][0][0])[hpos[k]] = nh[k][c];
+      }
+    const R rz = nr;
     __syncthreads();
-    if (ix < nx && iy < ny) {
+    issue(z + kCzAhead);
+    if (z + 1 < ze) fetch(z + 1);
+    if (own) {
       const V3<R> Bm = {q[0][RI], q[1][RI], q[2][RI]};
       R g[3][3];
       V3<R> hod = {0, 0, 0};
@@ -454,7 +538,7 @@ __global__ void __launch_bounds__(kCzTX * kCzTY) k_curl_e_z(const __grid_constan
           R b3[3];
 #pragma unroll
           for (int c = 0; c < 3; ++c)
-            b3[c] = ax == 0 ? pl[c][ty + RI][tx + RI + o] : (ax == 1 ? pl[c][ty + RI + o][tx + RI] : q[c][RI + o]);
+            b3[c] = ax == 0 ? P[c][ty + RI][tx + RI + o] : (ax == 1 ? P[c][ty + RI + o][tx + RI] : q[c][RI + o]);
           const R cH = a.Hint[o + RI];
           if (o == 0) {
             if (HODS) {
@@ -478,13 +562,12 @@ __global__ void __launch_bounds__(kCzTX * kCzTY) k_curl_e_z(const __grid_constan
       const long long idx = ix + (long long)nx * iy + sz * z;
       V3<R> J = {g[1][2] - g[2][1], g[2][0] - g[0][2], g[0][1] - g[1][0]};
       if (a.rho) {
-        const R r = (R)1 / __ldg(a.rho + idx);
+        const R r = (R)1 / rz;
         J = {J.x * r, J.y * r, J.z * r};
       }
       stf(a.out, idx, V3<R>{J.x * Bm.y - J.y * Bm.x, J.x * Bm.z - J.z * Bm.x, J.y * Bm.z - J.z * Bm.y});
       if (HODS) stf(a.hout, idx, hod);
     }
-    __syncthreads();
   }
 }
 
