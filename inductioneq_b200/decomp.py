@@ -1,15 +1,25 @@
-"""Domain decomposition of one periodic solve into z slabs, one slab per rank (one process
-per GPU).
+"""Domain decomposition of one solve into z slabs, one slab per rank (one process per GPU).
 
 The reference runs one grid on one device (matlab/+induction_eq/initialize.m:31-34); its
 paper sweeps go to 320^3 and beyond (paper/convergence_rotation_3D.m:104).  Here rank k of
 P owns the contiguous planes [z0_k, z1_k) of the global grid -- in the reference layout,
-idx = ix + NX*(iy + NY*iz), a z slab is one contiguous block of memory -- and holds G ghost
-planes on each side, G = 2 * (ORDER/2): the Hall term reaches ORDER/2 planes for curl(B)/rho
-and ORDER/2 more for the flux rows of E = J x B, the volume, dissipation and convection terms
-reach ORDER/2.  The rank's context is the global settings with NODES_Z = (z1_k - z0_k) + 2G,
-the global spacing, the grid periodic, and the slab's z offset, so that testcase coordinates
-(init, u_analytical, analytical_b) are those of the global grid.
+idx = ix + NX*(iy + NY*iz), a z slab is one contiguous block of memory -- and holds ghost
+planes beside its owned ones.  The rank's context is the global settings with NODES_Z = the
+slab's planes (ghosts included), the global spacing and the slab's z offset, so that testcase
+coordinates (init, u_analytical, analytical_b, b_boundary) are those of the global grid.
+
+Periodic grids: G = 2 * (ORDER/2) ghost planes on each side of every slab -- the Hall term
+reaches ORDER/2 planes for curl(B)/rho and ORDER/2 more for the flux rows of E = J x B, the
+volume, dissipation and convection terms reach ORDER/2 -- and the slab is itself periodic:
+the rows that wrap at its ends are ghost rows.
+
+Boxes (non-periodic): no ghost planes at the global ends (the slab's end is the box's face,
+with its SBP boundary rows and SAT terms); G = NUM_BOUNDS + ORDER/2 ghost planes at an end
+inside the grid.  The slab is an ordinary box of the stencil kernels: its own boundary rows
+and face terms at an inner end fall on the ghost planes only, every owned node is at least
+NUM_BOUNDS planes from that end (an interior row, as in the global grid), and every value
+of curl(B)/rho an owned node reads (ORDER/2 planes away) is itself formed by an interior row
+from valid ghost values.  So the box kernels run unchanged on the slab.
 
 A step runs the integrator on the local slab either through the context's fused stage kernels,
 one RK stage at a time (ieq_stages_*: the ghost planes of the state fields are refreshed after
@@ -17,15 +27,13 @@ every stage), or as the reference's kernel list (compute_numerical_solution_setu
 After every stage -- every kernel of the list that writes a state field (all but
 calc_curlB_rho_*, calc_u_* and calc_time_*) -- the state fields' ghost planes are refreshed from
 the neighbours' owned planes: the G planes at the bottom of the owned range go to the rank
-below, the G at the top to the rank above, periodically (rank 0's lower neighbour is rank
+below, the G at the top to the rank above (periodic grids: rank 0's lower neighbour is rank
 P-1) -- one point-to-point exchange per neighbour and field (NCCL between GPUs, gloo on CPU).
 curl(B)/rho is recomputed on every local plane from fresh ghosts, so it is never exchanged;
-its values within ORDER/2 of the slab's ends are not valid and are never read by an owned
-node.  Each owned node then performs exactly the arithmetic of the undecomposed run, so the
-decomposed fields equal it bit for bit.
-
-Non-periodic boxes are not decomposed here: their slabs would need SBP boundary rows in x and
-y but interior rows in z, a combination the stencil kernels do not instantiate.
+its values near the slab's inner ends are not valid and are never read by an owned node.
+Each owned node then performs exactly the arithmetic of the undecomposed run, so the
+decomposed fields equal it bit for bit.  `run_local` runs the slabs of several ranks in one
+process on one device, stage by stage, with the ghost planes copied between their buffers.
 """
 from __future__ import annotations
 
@@ -53,22 +61,32 @@ def slab_bounds(nz: int, world: int) -> list[tuple[int, int]]:
 
 @dataclass
 class ZSlabs:
-    """One rank's view of the decomposition of a periodic (nx, ny, nz) grid."""
+    """One rank's view of the decomposition of an (nx, ny, nz) grid: `ghosts` planes at every
+    slab end of a periodic grid, at the ends inside the grid of a box."""
     ranks: Ranks
     nx: int
     ny: int
     nz: int
     ghosts: int
+    periodic: bool = True
 
     def __post_init__(self):
-        w = self.ranks.world
+        w, r = self.ranks.world, self.ranks.rank
         self.bounds = slab_bounds(self.nz, w)
-        self.z0, self.z1 = self.bounds[self.ranks.rank]
-        if min(b - a for a, b in self.bounds) < self.ghosts:
+        self.z0, self.z1 = self.bounds[r]
+        if w > 1 and min(b - a for a, b in self.bounds) < self.ghosts:
             raise ValueError(f"every rank must own at least {self.ghosts} planes (the ghost depth): "
                              f"{self.nz} planes over {w} ranks")
-        self.up = (self.ranks.rank + 1) % w
-        self.down = (self.ranks.rank - 1) % w
+        if self.periodic:
+            if self.owned < self.ghosts:
+                raise ValueError(f"a periodic slab must own at least {self.ghosts} planes (the ghost depth)")
+            self.g_lo = self.g_hi = self.ghosts
+            self.up, self.down = (r + 1) % w, (r - 1) % w
+        else:
+            self.g_lo = self.ghosts if r > 0 else 0
+            self.g_hi = self.ghosts if r < w - 1 else 0
+            self.up = r + 1 if r < w - 1 else None
+            self.down = r - 1 if r > 0 else None
 
     @property
     def owned(self) -> int:
@@ -76,7 +94,7 @@ class ZSlabs:
 
     @property
     def nloc(self) -> int:
-        return self.owned + 2 * self.ghosts
+        return self.owned + self.g_lo + self.g_hi
 
     @property
     def plane(self) -> int:
@@ -89,50 +107,77 @@ class ZSlabs:
     @property
     def z_offset(self) -> int:
         """Global plane of local plane 0."""
-        return self.z0 - self.ghosts
+        return self.z0 - self.g_lo
 
     def scatter(self, glob: np.ndarray) -> np.ndarray:
         """The local slab (ghosts included) of a global field in the reference layout
-        ((N,) or (N, C) rows, N = nx*ny*nz), periodic in z."""
+        ((N,) or (N, C) rows, N = nx*ny*nz); periodic grids wrap in z."""
         g = glob[: self.nz * self.plane].reshape((self.nz, self.plane) + glob.shape[1:])
         zs = np.arange(self.z_offset, self.z_offset + self.nloc) % self.nz
         return np.ascontiguousarray(g[zs].reshape((self.nloc * self.plane,) + glob.shape[1:]))
 
     def owned_rows(self) -> slice:
         """Rows of the owned planes in a local field."""
-        return slice(self.ghosts * self.plane, (self.ghosts + self.owned) * self.plane)
+        return slice(self.g_lo * self.plane, (self.g_lo + self.owned) * self.plane)
 
     def global_rows(self) -> slice:
         """Rows of the owned planes in the global field."""
         return slice(self.z0 * self.plane, self.z1 * self.plane)
+
+    def parts(self, t):
+        """(lower ghosts, lowest G owned planes, highest G owned planes, upper ghosts) of a
+        local field (rows in the reference layout)."""
+        G, P, n, lo = self.ghosts, self.plane, self.owned, self.g_lo
+        return (t[0: lo * P], t[lo * P: (lo + G) * P], t[(lo + n - G) * P: (lo + n) * P],
+                t[(lo + n) * P: (lo + n + self.g_hi) * P])
 
     def exchange(self, *fields) -> None:
         """Refresh the ghost planes of every field (torch tensors or numpy arrays over the
         local slab, rows in the reference layout; padded rows beyond the slab are ignored)
         from the neighbours' owned planes."""
         import torch
-        G, P, n = self.ghosts, self.plane, self.owned
         for f in fields:
             t = torch.from_numpy(f) if isinstance(f, np.ndarray) else f
-            lo_ghost = t[0: G * P]
-            lo_owned = t[G * P: 2 * G * P]
-            hi_owned = t[n * P: (n + G) * P]
-            hi_ghost = t[(n + G) * P: (n + 2 * G) * P]
+            lo_ghost, lo_owned, hi_owned, hi_ghost = self.parts(t)
             if self.ranks.world == 1:
-                lo_ghost.copy_(hi_owned)
-                hi_ghost.copy_(lo_owned)
+                if self.periodic:
+                    lo_ghost.copy_(hi_owned)
+                    hi_ghost.copy_(lo_owned)
                 continue
             import torch.distributed as dist
-            send_lo, send_hi = lo_owned.contiguous(), hi_owned.contiguous()
-            recv_hi, recv_lo = torch.empty_like(hi_ghost), torch.empty_like(lo_ghost)
-            # posted in this order on every rank: with two ranks (up == down) the first
-            # message between a pair is the sender's bottom block, the receiver's top ghosts
-            ops = [dist.P2POp(dist.isend, send_lo, self.down), dist.P2POp(dist.isend, send_hi, self.up),
-                   dist.P2POp(dist.irecv, recv_hi, self.up), dist.P2POp(dist.irecv, recv_lo, self.down)]
+            ops, recv = [], []
+            # posted in this order on every rank: with two periodic ranks (up == down) the
+            # first message between a pair is the sender's bottom block, the receiver's top
+            # ghosts
+            if self.down is not None:
+                ops.append(dist.P2POp(dist.isend, lo_owned.contiguous(), self.down))
+            if self.up is not None:
+                ops.append(dist.P2POp(dist.isend, hi_owned.contiguous(), self.up))
+            if self.up is not None:
+                rh = torch.empty_like(hi_ghost)
+                ops.append(dist.P2POp(dist.irecv, rh, self.up))
+                recv.append((hi_ghost, rh))
+            if self.down is not None:
+                rl = torch.empty_like(lo_ghost)
+                ops.append(dist.P2POp(dist.irecv, rl, self.down))
+                recv.append((lo_ghost, rl))
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-            hi_ghost.copy_(recv_hi)
-            lo_ghost.copy_(recv_lo)
+            for dst, src in recv:
+                dst.copy_(src)
+
+
+def exchange_local(slabs: list, fields: list) -> None:
+    """The ghost exchange of the ranks of one decomposition held in one process: slabs[k] is
+    rank k's ZSlabs, fields[k] its list of local fields (the same fields in the same order on
+    every rank); every ghost block is copied from the neighbour's owned planes."""
+    for i in range(len(fields[0])):
+        parts = [sl.parts(f[i]) for sl, f in zip(slabs, fields)]
+        for k, sl in enumerate(slabs):
+            if sl.down is not None:
+                parts[k][0].copy_(parts[sl.down][2])
+            if sl.up is not None:
+                parts[k][3].copy_(parts[sl.up][1])
 
 
 def exchanges_after(kernel: str) -> bool:
@@ -160,12 +205,16 @@ def decomposed_steps(slabs: ZSlabs, runner, seq, num_steps: int, state, args, sy
                     sync()
 
 
+def is_periodic(maps) -> bool:
+    return maps.I_RunOps.get("periodic") == "USE_PERIODIC"
+
+
 def local_maps(maps, slabs: ZSlabs):
     """The settings of one rank's slab: the global maps with NODES_Z = the slab's planes
-    including ghosts, the global spacing and the slab's z offset (periodic grids only)."""
+    including ghosts, the global spacing and the slab's z offset."""
     import copy
-    if maps.I_RunOps.get("periodic") != "USE_PERIODIC":
-        raise ValueError("the z-slab decomposition needs a periodic grid")
+    if is_periodic(maps) != slabs.periodic:
+        raise ValueError("the slabs and the settings disagree on whether the grid is periodic")
     m = copy.deepcopy(maps)
     m.spacing_override = maps.spacing()
     m.I_Mesh["NODES_Z"] = slabs.nloc
@@ -174,10 +223,20 @@ def local_maps(maps, slabs: ZSlabs):
     return m
 
 
-def ghost_depth(order: int) -> int:
-    """Ghost planes a slab needs for one stage: ORDER/2 for curl(B)/rho and ORDER/2 for the
-    flux rows of E (the interior rows of a periodic grid)."""
-    return 2 * (order // 2)
+# NUM_BOUNDS (boundary rows at each end) of the SBP operators (include/*Order*.h), by
+# (order, extended)
+NUM_BOUNDS = {(2, False): 1, (4, False): 4, (6, False): 6, (2, True): 3, (4, True): 6, (6, True): 8}
+
+
+def ghost_depth(order: int, periodic: bool = True, extended: bool = False) -> int:
+    """Ghost planes a slab needs at an end for one stage.  Periodic grids: ORDER/2 for
+    curl(B)/rho and ORDER/2 for the flux rows of E (interior rows everywhere).  Boxes, at an
+    end inside the grid: NUM_BOUNDS, so that the slab's own boundary rows there cover ghost
+    planes only, plus ORDER/2, so that the curl(B)/rho values an owned node reads are formed
+    by interior rows."""
+    if periodic:
+        return 2 * (order // 2)
+    return NUM_BOUNDS[(order, extended)] + order // 2
 
 
 TWO_FIELD_INTEGRATORS = ("CarpenterKennedy2N54", "ToulorgeDesmet2N84F")
@@ -192,16 +251,19 @@ class _DeviceArray:
 
 
 class SlabSolve:
-    """One rank's slab of a decomposed periodic solve on its GPU: the local context (the C
-    ABI's reference kernels, ieq_run_kernels) on torch device buffers, the ghost exchanges
-    through torch.distributed (NCCL between GPUs; a local copy with one rank)."""
+    """One rank's slab of a decomposed solve (periodic grid or box) on its GPU: the local
+    context (fused stage kernels or the C ABI's reference kernels) on torch device buffers,
+    the ghost exchanges through torch.distributed (NCCL between GPUs; a local copy with one
+    periodic rank), or between the slabs of one process with `run_local`."""
 
     def __init__(self, maps, ranks: Ranks, device: int = 0):
         import torch
         m = maps.I_Mesh
         self.ranks = ranks
+        per = is_periodic(maps)
+        ext = maps.I_RunOps.get("operator_form", "classical") == "extended"
         self.slabs = ZSlabs(ranks, int(m["NODES_X"]), int(m["NODES_Y"]), int(m["NODES_Z"]),
-                            ghost_depth(int(maps.I_RunOps["order"])))
+                            ghost_depth(int(maps.I_RunOps["order"]), per, ext), per)
         self.device = device
         self.ctx = local_maps(maps, self.slabs).context(device)
         self.seq = self.ctx.step_kernels()
@@ -293,3 +355,52 @@ class SlabSolve:
     def close(self) -> None:
         self.__dict__.pop("_views", None)   # views of the context's memory
         self.ctx.close()
+
+
+def run_local(solves: list, num_steps: int, fused: bool = True) -> None:
+    """num_steps steps of a decomposition whose ranks' slabs (SlabSolve, ranks 0..P-1 of one
+    Ranks world, every slab on the same device) live in one process: every stage (fused) or
+    every state-writing kernel of the list runs on each slab in turn, the slabs' devices are
+    synchronised, and the ghost planes are copied between the slabs' buffers."""
+    import torch
+    slabs = [s.slabs for s in solves]
+
+    def sync():
+        for s in solves:
+            s._sync()
+
+    sync()
+    if not fused:
+        seq = solves[0].seq
+        for _ in range(num_steps):
+            for k in seq:
+                for s in solves:
+                    s.ctx.run(k, s.slabs.local_nodes, *s.args)
+                if exchanges_after(k):
+                    sync()
+                    exchange_local(slabs, [s.state for s in solves])
+                    torch.cuda.synchronize(solves[0].device)
+        sync()
+        return
+    parts = []
+    for s in solves:
+        a = s.args
+        b3 = a[2] if s.nf == 3 else None
+        cb, u = (a[3], a[4]) if s.nf == 3 else (a[2], a[3])
+        parts.append((a, b3, cb, u, a[-2], a[-1]))
+    begun = []
+    try:
+        for s, (a, b3, cb, u, rho, time) in zip(solves, parts):
+            ns = s.ctx.stages_begin(a[0], a[1], b3, cb, u)
+            begun.append(s)
+        for _ in range(num_steps):
+            for st in range(ns):
+                for s, (a, b3, cb, u, rho, time) in zip(solves, parts):
+                    s.ctx.stages_run(rho, time, st)
+                sync()
+                exchange_local(slabs, [s._stage_planes() for s in solves])
+                torch.cuda.synchronize(solves[0].device)
+    finally:
+        for s, (a, b3, cb, u, rho, time) in zip(begun, parts):
+            s.ctx.stages_end(a[0], a[1], b3, cb, u, rho)
+        sync()

@@ -74,6 +74,11 @@ class OracleConfig:
     cmax: float = 10.0
     tc_omega: float = 1.0
     bnodes: int = 1
+    # a z slab of a decomposed grid of nzg planes whose plane 0 is global plane zoff: testcase
+    # coordinates are the global grid's (IEQ_Z_OFFSET / IEQ_NZ_GLOBAL of the CUDA library;
+    # not a reference setting -- the reference runs one grid); nzg = 0: the whole domain
+    zoff: int = 0
+    nzg: int = 0
 
     def spacing(self):
         # matlab/+induction_eq/initialize.m:12-21
@@ -160,7 +165,8 @@ class NumpyOracle:
         T = self.T
         x = (T(c.xmin[0]) + self._coord[0].astype(T) * T(self.d[0]))[None, None, :]
         y = (T(c.xmin[1]) + self._coord[1].astype(T) * T(self.d[1]))[None, :, None]
-        z = (T(c.xmin[2]) + self._coord[2].astype(T) * T(self.d[2]))[:, None, None]
+        gz = self._coord[2] if c.nzg <= 0 else np.mod(self._coord[2] + c.zoff, c.nzg)
+        z = (T(c.xmin[2]) + gz.astype(T) * T(self.d[2]))[:, None, None]
         return x, y, z
 
     def _v4(self, a, b, c, d=None):

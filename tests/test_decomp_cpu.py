@@ -1,11 +1,14 @@
-"""The z-slab decomposition of one periodic solve (inductioneq_b200.decomp) on CPU ranks.
+"""The z-slab decomposition of one solve (inductioneq_b200.decomp) on CPU ranks.
 
 Every rank (a spawned process, gloo) runs the integrator's kernel list on its slab with the
 oracle as the per-rank engine and exchanges the ghost planes of the state fields between
 kernels; the owned planes of every rank must equal the single-process run of the whole grid
-bit for bit (each owned node performs the same arithmetic).  Two ranks (the upper and lower
-neighbour are the same rank) and three ranks (different neighbours), Hall + high-order
-dissipation with CarpenterKennedy2N54 and Hall with a constant velocity with SSPRK33.
+bit for bit (each owned node performs the same arithmetic).  Two ranks and three ranks
+(different neighbours); periodic grids (with two ranks the upper and lower neighbour are the
+same rank: Hall + high-order dissipation with CarpenterKennedy2N54, Hall with a constant
+velocity with SSPRK33) and boxes (no ghosts at the box's z faces, NUM_BOUNDS + ORDER/2 at
+the inner slab ends: rotation with SAT inflow and SSPRK33, confined Hall with high-order
+dissipation and CarpenterKennedy2N54, an extended operator).
 """
 from __future__ import annotations
 
@@ -27,14 +30,27 @@ CASES = {
                                steps=2),
     "hallper_2c_conv_ssp": dict(order=2, testcase="hall_periodic", nodes=(7, 8, 9), lo=0.0, hi=HP, hall=True,
                                 integrator="SSPRK33", dt=0.005, steps=2),
+    "rot3d_4c_ssp_box": dict(order=4, testcase="rotation_3D", nodes=(8, 9, 30), lo=-1.0, hi=1.0, periodic=False,
+                             integrator="SSPRK33", dt=0.005, steps=2),
+    "confined_6c_hall_hod_ck_box": dict(order=6, testcase="confined_domain", nodes=(9, 8, 30), lo=0.0, hi=1.0,
+                                        periodic=False, hall=True, dissipation="HIGH_ORDER",
+                                        integrator="CarpenterKennedy2N54", dt=1e-5, steps=2),
+    "confined_4e_hall_ck_box": dict(order=4, extended=True, testcase="confined_domain", nodes=(8, 7, 25), lo=0.0,
+                                    hi=1.0, periodic=False, hall=True, integrator="CarpenterKennedy2N54", dt=1e-5,
+                                    steps=2),
 }
 
 
-def _oracle(c, nodes):
+def _ghosts(c):
+    return D.ghost_depth(c["order"], c.get("periodic", True), c.get("extended", False))
+
+
+def _oracle(c, nodes, zoff=0, nzg=0):
     from oracle.numpy_oracle import NumpyOracle, OracleConfig
-    cfg = OracleConfig(nodes=nodes, xmin=(c["lo"],) * 3, xmax=(c["hi"],) * 3, order=c["order"], periodic=True,
+    cfg = OracleConfig(nodes=nodes, xmin=(c["lo"],) * 3, xmax=(c["hi"],) * 3, order=c["order"],
+                       extended=c.get("extended", False), periodic=c.get("periodic", True),
                        hall=c.get("hall", False), dissipation=c.get("dissipation", "NONE"), testcase=c["testcase"],
-                       dt=c["dt"])
+                       dt=c["dt"], zoff=zoff, nzg=nzg)
     return NumpyOracle(cfg)
 
 
@@ -64,8 +80,8 @@ def _rank_run(rk: R.Ranks, c: dict):
     try:
         g, b, u = _initial(c)
         nx, ny, nz = c["nodes"]
-        slabs = D.ZSlabs(rk, nx, ny, nz, D.ghost_depth(c["order"]))
-        o = _oracle(c, slabs.local_nodes)
+        slabs = D.ZSlabs(rk, nx, ny, nz, _ghosts(c), c.get("periodic", True))
+        o = _oracle(c, slabs.local_nodes, slabs.z_offset, nz)
         o.d = g.d   # the global spacing
         nf = NUM_FIELDS[c["integrator"]]
         lb, lu = slabs.scatter(b), slabs.scatter(u)
@@ -115,7 +131,7 @@ def _spawn(world, case):
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_decomposed_solve_equals_single_process_run(world, case):
     c = CASES[case]
-    if world == 3 and c["nodes"][2] < 3 * D.ghost_depth(c["order"]):
+    if world == 3 and c["nodes"][2] < 3 * _ghosts(c):
         pytest.skip("grid too short for three slabs of this ghost depth")
     out = _spawn(world, case)
     for r, v in out.items():
@@ -160,3 +176,36 @@ def test_local_maps_keep_the_global_spacing_and_offset():
     m.I_RunOps["periodic"] = "NONE"
     with pytest.raises(ValueError):
         D.local_maps(m, sl)
+
+
+def test_box_slabs_have_ghosts_only_at_inner_ends():
+    G = D.ghost_depth(6, periodic=False)
+    assert G == 6 + 3 and D.ghost_depth(4, periodic=False, extended=True) == 6 + 2
+    sl = [D.ZSlabs(R.Ranks(3, r, r), 8, 8, 40, G, periodic=False) for r in range(3)]
+    assert [(s.g_lo, s.g_hi) for s in sl] == [(0, G), (G, G), (G, 0)]
+    assert [s.z_offset for s in sl] == [0, 14 - G, 27 - G]
+    assert sl[0].down is None and sl[2].up is None and sl[1].down == 0 and sl[1].up == 2
+    assert sl[2].nloc == sl[2].owned + G
+    # one rank: the whole box, no ghosts
+    one = D.ZSlabs(R.Ranks(1, 0, 0), 8, 8, 40, G, periodic=False)
+    assert (one.g_lo, one.g_hi, one.nloc) == (0, 0, 40)
+    glob = np.arange(8 * 8 * 40, dtype=np.float64)
+    np.testing.assert_array_equal(sl[1].scatter(glob), glob[(14 - G) * 64:(27 + G) * 64])
+
+
+def test_local_exchange_fills_ghosts_from_neighbours():
+    import torch
+    G = D.ghost_depth(2, periodic=False)
+    for periodic in (False, True):
+        g = D.ghost_depth(2) if periodic else G
+        sl = [D.ZSlabs(R.Ranks(3, r, r), 2, 2, 12, g, periodic=periodic) for r in range(3)]
+        glob = np.arange(2 * 2 * 12, dtype=np.float64)
+        loc = [torch.from_numpy(s.scatter(glob)) for s in sl]
+        want = [t.clone() for t in loc]
+        for s, t in zip(sl, loc):
+            lo, _, _, hi = s.parts(t)
+            lo.fill_(-1.0)
+            hi.fill_(-1.0)
+        D.exchange_local(sl, [[t] for t in loc])
+        for t, w in zip(loc, want):
+            assert torch.equal(t, w)

@@ -1,10 +1,13 @@
-"""The z-slab decomposition on the GPU with one rank: the slab (the whole grid plus ghost
-planes refreshed by a local copy) runs the fused stage kernels one RK stage at a time
-(ieq_stages_*) or the reference kernel lists through the C ABI on torch device buffers; its
-owned planes equal the undecomposed run of the same kernels bit for bit.  The
+"""The z-slab decomposition on the GPU: a slab (ghost planes refreshed by copies) runs the
+fused stage kernels one RK stage at a time (ieq_stages_*) or the reference kernel lists
+through the C ABI on torch device buffers; its owned planes equal the undecomposed run of the
+same kernels bit for bit.  One slab (a periodic grid's ghosts wrap onto the slab itself), and
+the 2 or 3 slabs of a decomposition held in one process on this GPU (`run_local`: every stage
+runs on each slab in turn, then the ghost planes are copied between their buffers) -- periodic
+grids and boxes, whose slabs carry ghost planes only at their inner ends.  The
 variable-velocity case checks that the slab's testcase coordinates are the global grid's
-(IEQ_Z_OFFSET / IEQ_NZ_GLOBAL).  Several ranks are covered on CPU (tests/test_decomp_cpu.py);
-this run has one GPU."""
+(IEQ_Z_OFFSET / IEQ_NZ_GLOBAL).  Several processes are covered on CPU
+(tests/test_decomp_cpu.py); this run has one GPU."""
 from __future__ import annotations
 
 import math
@@ -13,7 +16,7 @@ import numpy as np
 import pytest
 
 from inductioneq_b200 import ranks as R
-from inductioneq_b200.decomp import SlabSolve
+from inductioneq_b200.decomp import SlabSolve, run_local
 from tests.helpers import maps_for
 
 pytestmark = pytest.mark.gpu
@@ -25,6 +28,33 @@ CASES = {
     "hallper_4c_varu_ssp": dict(order=4, testcase="hall_periodic", nodes=(12, 14, 16), lo=0.0, hi=4 * math.pi / 3,
                                 periodic=True, hall=True, integrator="SSPRK33", dt=0.002, variable_u=True),
 }
+
+# boxes: the rotation with SAT inflow (convection pair kernels, x band) and the confined Hall
+# box with the dissipation sum and the Hall outflow SAT
+BOX_CASES = {
+    "rot3d_4c_ssp_box": dict(order=4, testcase="rotation_3D", nodes=(40, 14, 36), lo=-1.0, hi=1.0,
+                             integrator="SSPRK33", dt=0.005),
+    "confined_6c_hall_hod_ck_box": dict(order=6, testcase="confined_domain", nodes=(16, 12, 40), lo=0.0, hi=1.0,
+                                        hall=True, dissipation="HIGH_ORDER", integrator="CarpenterKennedy2N54",
+                                        dt=1e-5),
+}
+
+
+def _undecomposed(c, fused, steps):
+    g = maps_for(dict(c, stage_kernel="AUTO" if fused else "LIST")).context()
+    b, u = g.vec(), g.vec()
+    g.kernel("init_b", b)
+    g.kernel("init_u", u)
+    bh = g.get_vec(b)
+    bh[: g.n, :3] += 1e-2 * np.random.default_rng(3).standard_normal((g.n, 3))
+    uh = g.get_vec(u)
+    dev = [g.vec(bh), g.vec(), g.vec(), g.vec(), g.vec(uh), g.scalar(np.ones(g.n_pad)), g.scalar(np.zeros(2), n=2)]
+    g.time_steps(*dev, steps)
+    ref = [g.get_vec(dev[i])[: g.n] for i in range(3)]
+    t_ref = g.get_scalar(dev[6], n=2)
+    n = g.n
+    g.close()
+    return bh[:n], uh[:n], ref, t_ref
 
 
 @pytest.mark.parametrize("fused", [False, True])
@@ -56,6 +86,35 @@ def test_single_slab_equals_undecomposed_run(name, fused):
     np.testing.assert_array_equal(s.time.cpu().numpy(), t_ref)
     s.close()
     g.close()
+
+
+@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("name", sorted(BOX_CASES) + ["whistler_6c_hod_ck"])
+def test_slabs_of_one_process_equal_undecomposed_run(name, world, fused):
+    c = BOX_CASES.get(name) or CASES[name]
+    steps = 3
+    bh, uh, ref, t_ref = _undecomposed(c, fused, steps)
+    solves = [SlabSolve(maps_for(c), R.Ranks(world, r, r)) for r in range(world)]
+    try:
+        if not c.get("periodic"):
+            assert solves[0].slabs.g_lo == 0 and solves[-1].slabs.g_hi == 0
+        for s in solves:
+            s.load(bh, uh, np.ones(bh.shape[0]))
+        run_local(solves, steps, fused=fused)
+        covered = 0
+        for s in solves:
+            rows = s.slabs.global_rows()
+            np.testing.assert_array_equal(s.owned(s.b), ref[0][rows])
+            np.testing.assert_array_equal(s.owned(s.b2), ref[1][rows])
+            if s.nf == 3:
+                np.testing.assert_array_equal(s.owned(s.b3), ref[2][rows])
+            np.testing.assert_array_equal(s.time.cpu().numpy(), t_ref)
+            covered += rows.stop - rows.start
+        assert covered == bh.shape[0]
+    finally:
+        for s in solves:
+            s.close()
 
 
 def test_stage_api_refuses_misuse():
