@@ -148,6 +148,12 @@ ieq_status ieq_norm2_diff_value(ieq_ctx *ctx, const void *vec_a, const void *vec
                                 double *result);
 ieq_status ieq_norm2_S_value(ieq_ctx *ctx, const void *scalar_field, double *result);
 ieq_status ieq_dot_value(ieq_ctx *ctx, const void *a, const void *b, double *result);
+/* The same unweighted dot product (kernel_dot_product.cl:47-74 summed like the host of
+ * clean_div.m:47-79) over the elements [first, first + count) of two scalar fields of the
+ * context's grid only: one rank's owned planes in a z-slab decomposition, whose per-rank
+ * sums are then added across the ranks.  IEQ_ERR_SHAPE if the range leaves the grid's nodes. */
+ieq_status ieq_dot_range(ieq_ctx *ctx, const void *a, const void *b, uint64_t first, uint64_t count,
+                         double *result);
 
 /* Result metrics of compute_numerical_solution.m:198-250 at time t: abs/rel L2 error
  * against b_analytical(t), ||div B|| and the energy.  work_vec/work_scalar are scratch

@@ -228,15 +228,38 @@ def local_maps(maps, slabs: ZSlabs):
 NUM_BOUNDS = {(2, False): 1, (4, False): 4, (6, False): 6, (2, True): 3, (4, True): 6, (6, True): 8}
 
 
-def ghost_depth(order: int, periodic: bool = True, extended: bool = False) -> int:
-    """Ghost planes a slab needs at an end for one stage.  Periodic grids: ORDER/2 for
-    curl(B)/rho and ORDER/2 for the flux rows of E (interior rows everywhere).  Boxes, at an
-    end inside the grid: NUM_BOUNDS, so that the slab's own boundary rows there cover ghost
-    planes only, plus ORDER/2, so that the curl(B)/rho values an owned node reads are formed
-    by interior rows."""
+LAPLACE_KEYS = {"WIDE_STENCIL_DIRICHLET": "WS_D0", "NARROW_STENCIL_DIRICHLET": "NS_D0", "WIDE_STENCIL_LNS": "WS_LN"}
+
+
+def laplace_rows(order: int, extended: bool, laplace: str) -> tuple[int, int]:
+    """(boundary rows at each end, stencil width) of the divergence cleaning's Laplacian
+    (kernel_div_cleaning.cl:11-56 on the include/*Order*.h tables)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "sbp_tables.json")) as f:
+        t = json.load(f)
+    lap = t[f"{order}{'e' if extended else 'c'}"]["laplace"][LAPLACE_KEYS[laplace]]
+    return int(lap["nb"]), int(lap["width"])
+
+
+def bnodes_of(laplace: str) -> int:
+    """BNODES: the Dirichlet layer the CG leaves at every face (0 for the LNS form)."""
+    return 0 if laplace == "WIDE_STENCIL_LNS" else 1
+
+
+def ghost_depth(order: int, periodic: bool = True, extended: bool = False,
+                laplace: str = "WIDE_STENCIL_DIRICHLET") -> int:
+    """Ghost planes a slab needs at an end.  Periodic grids: ORDER/2 for curl(B)/rho and
+    ORDER/2 for the flux rows of E (interior rows everywhere).  Boxes, at an end inside the
+    grid: NUM_BOUNDS, so that the slab's own boundary rows there cover ghost planes only, plus
+    ORDER/2, so that the curl(B)/rho values an owned node reads are formed by interior rows;
+    and at least the divergence cleaning's Laplacian boundary rows and reach and the CG's
+    Dirichlet layer, so that a decomposed cleaning gives every owned node the global grid's
+    rows too."""
     if periodic:
         return 2 * (order // 2)
-    return NUM_BOUNDS[(order, extended)] + order // 2
+    nb_l, w_l = laplace_rows(order, extended, laplace)
+    return max(NUM_BOUNDS[(order, extended)] + order // 2, nb_l, (w_l - 1) // 2, bnodes_of(laplace))
 
 
 TWO_FIELD_INTEGRATORS = ("CarpenterKennedy2N54", "ToulorgeDesmet2N84F")
@@ -262,11 +285,13 @@ class SlabSolve:
         self.ranks = ranks
         per = is_periodic(maps)
         ext = maps.I_RunOps.get("operator_form", "classical") == "extended"
+        self.laplace = maps.I_DC["divergence_cleaning_form"].replace("USE_LAPLACE_", "")
         self.slabs = ZSlabs(ranks, int(m["NODES_X"]), int(m["NODES_Y"]), int(m["NODES_Z"]),
-                            ghost_depth(int(maps.I_RunOps["order"]), per, ext), per)
+                            ghost_depth(int(maps.I_RunOps["order"]), per, ext, self.laplace), per)
         self.device = device
         self.ctx = local_maps(maps, self.slabs).context(device)
-        self.seq = self.ctx.step_kernels()
+        # the integrator's kernel list (none without an integrator: a slab only cleaned)
+        self.seq = self.ctx.step_kernels() if maps.I_TI.get("time_integrator") else []
         self.nf = 2 if maps.I_TI["time_integrator"] in TWO_FIELD_INTEGRATORS else 3
         dt = torch.float32 if self.ctx.real == np.float32 else torch.float64
         n = self.ctx.n_pad
@@ -348,6 +373,32 @@ class SlabSolve:
             views += cache[base]
         return views
 
+    def clean_div(self, max_iterations: int, absolute_error_threshold: float) -> dict:
+        """The divergence cleaning of a decomposed box (clean_div_decomposed) on this rank's
+        slab, collective over the ranks: ghost planes through torch.distributed, dot products
+        of the owned planes all-reduced in FP64."""
+        import torch
+        if self.slabs.periodic:
+            raise ValueError("the decomposed divergence cleaning runs on boxes")
+        parts = [(self.slabs, self.ctx, self.b, _cg_fields(self))]
+        dev = torch.device("cuda", self.device)
+
+        def total(vals):
+            v = float(sum(vals))
+            if self.ranks.world == 1:
+                return v
+            import torch.distributed as dist
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t)
+            return float(t.item())
+
+        def sync():
+            self._sync()
+
+        return clean_div_decomposed(parts, max_iterations, absolute_error_threshold, bnodes_of(self.laplace),
+                                    total=total, exchange=lambda f: self.slabs.exchange(*f[0]),
+                                    scalar=_device_scalar(self), sync=sync)
+
     def owned(self, field) -> np.ndarray:
         """The owned planes of a field as a host array (rows of the global planes z0..z1)."""
         return field[self.slabs.owned_rows()].cpu().numpy()
@@ -404,3 +455,111 @@ def run_local(solves: list, num_steps: int, fused: bool = True) -> None:
         for s, (a, b3, cb, u, rho, time) in zip(begun, parts):
             s.ctx.stages_end(a[0], a[1], b3, cb, u, rho)
         sync()
+
+
+def clean_div_decomposed(parts, max_iterations: int, absolute_error_threshold: float, bnodes: int,
+                         total, exchange, scalar, sync=None) -> dict:
+    """clean_div.m:36-79 -- the CG projection of B -- on a decomposed box, as the reference's
+    host loop over its kernels, run on every slab held here.
+
+    parts: one (ZSlabs, engine, b, cg) per slab of this process, cg a dict of the slab's
+    scalar fields div, phi, lap, r, u (zero on entry); engine.run(name, grange, *args) runs a
+    reference kernel on the slab, engine.dot_range(x, y, first, count) a dot product over
+    elements [first, first + count).  total(values) adds the slabs' values of all processes
+    (the owned planes partition the grid, so every dot product of the reference is the sum of
+    the slabs' dots over their owned planes; between processes an FP64 all-reduce, 2 per
+    iteration).  exchange(fields) refreshes the ghost planes (fields: one list per slab).
+    scalar(engine, value) makes the 1-element array a kernel takes for alpha or beta; sync()
+    orders the engines' device work against the exchanges.  Ghost planes: the CG direction u
+    once per iteration (the Laplacian reads it across the slab's ends), phi before the
+    projection (its gradient) and B after it.  Returns iterations, residual_norm2,
+    initial_norm and history (the residual before every iteration)."""
+    import math
+    sync = sync or (lambda: None)
+
+    def grid_dc(sl):
+        return (sl.nx - 2 * bnodes, sl.ny - 2 * bnodes, sl.nloc - 2 * bnodes)
+
+    def dot(x, y):
+        vals = []
+        for sl, eng, _, cg in parts:
+            vals.append(eng.dot_range(cg[x] if isinstance(x, str) else x, cg[y], sl.g_lo * sl.plane,
+                                      sl.owned * sl.plane))
+        return total(vals)
+
+    for sl, eng, b, cg in parts:
+        eng.run("calc_div_divcleaning", grid_dc(sl), b, cg["div"])
+    sync()
+    for sl, eng, b, cg in parts:
+        cg["r"][:] = cg["div"]
+    sync()
+    residual_norm2 = dot("r", "r")
+    old = 1.0
+    initial = math.sqrt(residual_norm2)
+    tol = absolute_error_threshold * absolute_error_threshold
+    it = 0
+    history = [residual_norm2]
+    while residual_norm2 > tol and it < max_iterations:
+        beta = residual_norm2 / old
+        for sl, eng, b, cg in parts:
+            eng.run("calc_axpy", grid_dc(sl), cg["u"], cg["r"], scalar(eng, beta))
+        sync()
+        exchange([[cg["u"]] for _, _, _, cg in parts])
+        sync()
+        for sl, eng, b, cg in parts:
+            eng.run("calc_laplace_divcleaning", grid_dc(sl), cg["u"], cg["lap"])
+        sync()
+        alpha = residual_norm2 / dot("u", "lap")
+        for sl, eng, b, cg in parts:
+            eng.run("calc_xpay", grid_dc(sl), cg["phi"], cg["u"], scalar(eng, alpha))
+            eng.run("calc_xpay", grid_dc(sl), cg["r"], cg["lap"], scalar(eng, -alpha))
+        sync()
+        old = residual_norm2
+        residual_norm2 = dot("r", "r")
+        history.append(residual_norm2)
+        it += 1
+    exchange([[cg["phi"]] for _, _, _, cg in parts])
+    sync()
+    for sl, eng, b, cg in parts:
+        eng.run("projector_divcleaning", sl.local_nodes, b, cg["phi"])
+    sync()
+    exchange([[b] for _, _, b, _ in parts])
+    sync()
+    return {"iterations": it, "residual_norm2": residual_norm2, "initial_norm": initial, "history": history}
+
+
+def _cg_fields(solve) -> dict:
+    import torch
+    dt = torch.float32 if solve.ctx.real == np.float32 else torch.float64
+    dev = torch.device("cuda", solve.device)
+    return {k: torch.zeros(solve.ctx.n_pad, dtype=dt, device=dev) for k in ("div", "phi", "lap", "r", "u")}
+
+
+def _device_scalar(solve):
+    import torch
+    dt = torch.float32 if solve.ctx.real == np.float32 else torch.float64
+
+    def make(_eng, v):
+        return torch.tensor([v], dtype=dt, device=torch.device("cuda", solve.device))
+    return make
+
+
+def clean_div_local(solves: list, max_iterations: int, absolute_error_threshold: float) -> dict:
+    """The decomposed divergence cleaning of the slabs of several ranks held in one process on
+    one device (SlabSolve, ranks 0..P-1 of one box decomposition): the slabs' dot products
+    added in rank order, ghost planes copied between their buffers."""
+    import torch
+    s0 = solves[0]
+    if s0.slabs.periodic:
+        raise ValueError("the decomposed divergence cleaning runs on boxes")
+    parts = [(s.slabs, s.ctx, s.b, _cg_fields(s)) for s in solves]
+
+    def sync():
+        for s in solves:
+            s._sync()
+        torch.cuda.synchronize(s0.device)
+
+    return clean_div_decomposed(parts, max_iterations, absolute_error_threshold, bnodes_of(s0.laplace),
+                                total=lambda v: float(sum(v)),
+                                exchange=lambda f: exchange_local([p[0] for p in parts], f),
+                                scalar=_device_scalar(s0), sync=sync)

@@ -84,6 +84,7 @@ def load() -> ctypes.CDLL:
         getattr(lib, f).argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double)]
     for f in ("ieq_norm2_diff_value", "ieq_dot_value"):
         getattr(lib, f).argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
+    lib.ieq_dot_range.argtypes = [vp, vp, vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
     lib.ieq_compute_results.argtypes = [vp, vp, ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_double * 4)]
     lib.ieq_check_finite.argtypes = [vp, vp]
     lib.ieq_test_brick_wait.argtypes = [vp, ctypes.c_int]
@@ -304,6 +305,12 @@ class Context:
     def dot(self, a, b) -> float:
         r = ctypes.c_double()
         self._check(self.lib.ieq_dot_value(self.h, _ptr(a), _ptr(b), ctypes.byref(r)))
+        return r.value
+
+    def dot_range(self, a, b, first: int, count: int) -> float:
+        """The dot product of elements [first, first + count) of two scalar fields."""
+        r = ctypes.c_double()
+        self._check(self.lib.ieq_dot_range(self.h, _ptr(a), _ptr(b), int(first), int(count), ctypes.byref(r)))
         return r.value
 
     def results(self, b, t: float, work_vec, work_scalar) -> dict:

@@ -209,3 +209,118 @@ def test_local_exchange_fills_ghosts_from_neighbours():
         D.exchange_local(sl, [[t] for t in loc])
         for t, w in zip(loc, want):
             assert torch.equal(t, w)
+
+
+# ----------------------------------------------------------------- decomposed divergence cleaning
+CLEAN_CASES = {
+    "confined_4c_ws_d0": dict(order=4, testcase="confined_domain", nodes=(12, 10, 30), lo=0.0, hi=1.0,
+                              periodic=False, laplace="WIDE_STENCIL_DIRICHLET", dt=1e-5),
+    "confined_6c_ns_d0": dict(order=6, testcase="confined_domain", nodes=(11, 12, 30), lo=0.0, hi=1.0,
+                              periodic=False, laplace="NARROW_STENCIL_DIRICHLET", dt=1e-5),
+    "confined_2c_ws_d0": dict(order=2, testcase="confined_domain", nodes=(10, 11, 21), lo=0.0, hi=1.0,
+                              periodic=False, laplace="WIDE_STENCIL_DIRICHLET", dt=1e-5),
+    "confined_2e_ws_ln": dict(order=2, extended=True, testcase="confined_domain", nodes=(10, 9, 24), lo=0.0,
+                              hi=1.0, periodic=False, laplace="WIDE_STENCIL_LNS", dt=1e-5),
+}
+CLEAN_ITERATIONS = 15
+
+
+def _clean_oracle(c, nodes, zoff=0, nzg=0):
+    from oracle.numpy_oracle import NumpyOracle, OracleConfig
+    cfg = OracleConfig(nodes=nodes, xmin=(c["lo"],) * 3, xmax=(c["hi"],) * 3, order=c["order"],
+                       extended=c.get("extended", False), periodic=False, testcase=c["testcase"], dt=c["dt"],
+                       laplace=c["laplace"], bnodes=D.bnodes_of(c["laplace"]), zoff=zoff, nzg=nzg)
+    return NumpyOracle(cfg)
+
+
+def _clean_initial(c):
+    o = _clean_oracle(c, c["nodes"])
+    b = o.vec()
+    o.run("init_b", o.cfg.nodes, b)
+    b[:, :3] += 1e-3 * np.random.default_rng(11).standard_normal((o.N, 3))
+    return o, b
+
+
+class _OracleEngine:
+    """The oracle as a slab's engine of the decomposed cleaning (the host's sum of the
+    per-item products of dot_product over a range)."""
+
+    def __init__(self, o):
+        self.o = o
+
+    def run(self, name, grange, *args):
+        self.o.run(name, grange, *args)
+
+    def dot_range(self, x, y, first, count):
+        return float(np.sum((x[first:first + count] * y[first:first + count]).astype(np.float64)))
+
+
+def _rank_clean(rk: R.Ranks, c: dict):
+    import torch
+    import torch.distributed as dist
+    R.init(rk, "gloo", timeout_s=60.0)
+    try:
+        g, b = _clean_initial(c)
+        nx, ny, nz = c["nodes"]
+        sl = D.ZSlabs(rk, nx, ny, nz, D.ghost_depth(c["order"], False, c.get("extended", False), c["laplace"]),
+                      periodic=False)
+        o = _clean_oracle(c, sl.local_nodes, sl.z_offset, nz)
+        o.d = g.d
+        lb = sl.scatter(b)
+        cg = {k: o.scalar() for k in ("div", "phi", "lap", "r", "u")}
+
+        def total(vals):
+            t = torch.tensor([float(sum(vals))], dtype=torch.float64)
+            dist.all_reduce(t)
+            return float(t.item())
+
+        res = D.clean_div_decomposed([(sl, _OracleEngine(o), lb, cg)], CLEAN_ITERATIONS, 1e-14,
+                                     D.bnodes_of(c["laplace"]), total=total,
+                                     exchange=lambda f: sl.exchange(*f[0]),
+                                     scalar=lambda _e, v: np.array([v], dtype=o.T))
+        rows = sl.owned_rows()
+        return {"z": (sl.z0, sl.z1), "b": lb[rows].copy(), "phi": cg["phi"][rows].copy(), "res": res}
+    finally:
+        R.finish(rk)
+
+
+def _clean_worker(rank, world, port, case, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(world),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    try:
+        q.put((rank, _rank_clean(R.Ranks.from_env(), CLEAN_CASES[case])))
+    except Exception as e:
+        q.put((rank, ("error", type(e).__name__, str(e)[:300])))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("case", sorted(CLEAN_CASES))
+def test_decomposed_cleaning_equals_single_process_cleaning(world, case):
+    # the same CG iterations and residual history, B and phi on the owned planes equal up to
+    # the order of the dot products' sums (the slabs' sums added across the ranks)
+    import torch.multiprocessing as mp
+    from oracle.hostloops import clean_div
+    c = CLEAN_CASES[case]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_clean_worker, args=(r, world, port, case, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=30)
+    for v in out.values():
+        assert not (isinstance(v, tuple) and v and v[0] == "error"), v
+    o, b = _clean_initial(c)
+    ref = clean_div(o, b, CLEAN_ITERATIONS, 1e-14, D.bnodes_of(c["laplace"]))
+    plane = c["nodes"][0] * c["nodes"][1]
+    scale = np.abs(b[: o.N, :3]).max()
+    pscale = np.abs(ref["phi"][: o.N]).max()
+    for v in out.values():
+        assert v["res"]["iterations"] == ref["iterations"] == CLEAN_ITERATIONS
+        np.testing.assert_allclose(v["res"]["history"], ref["history"], rtol=1e-10)
+        rows = slice(v["z"][0] * plane, v["z"][1] * plane)
+        assert np.abs(v["b"][:, :3] - b[rows, :3]).max() <= 1e-12 * scale
+        assert np.abs(v["phi"] - ref["phi"][rows]).max() <= 1e-10 * pscale
+    assert ref["history"][-1] < 1e-2 * ref["history"][0]

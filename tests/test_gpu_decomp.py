@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from inductioneq_b200 import ranks as R
-from inductioneq_b200.decomp import SlabSolve, run_local
+from inductioneq_b200.decomp import SlabSolve, clean_div_local, run_local
 from tests.helpers import maps_for
 
 pytestmark = pytest.mark.gpu
@@ -115,6 +115,66 @@ def test_slabs_of_one_process_equal_undecomposed_run(name, world, fused):
     finally:
         for s in solves:
             s.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("laplace", ["WIDE_STENCIL_DIRICHLET", "NARROW_STENCIL_DIRICHLET", "WIDE_STENCIL_LNS"])
+def test_decomposed_cleaning_equals_undecomposed_cleaning(laplace, world):
+    # clean_div.m's CG through the reference kernels on 2 or 3 slabs of a confined box (ghost
+    # planes of u, phi and B copied between the slabs, dot products of the owned planes by
+    # ieq_dot_range added in rank order) against the same host loop on the whole grid: the
+    # same iterations and residual history, B equal up to the order of the dots' sums
+    c = dict(order=4, testcase="confined_domain", nodes=(24, 20, 36), lo=0.0, hi=1.0, hall=True, dt=1e-5,
+             laplace=laplace)
+    iters, thr = 25, 1e-14
+    g = maps_for(c).context()
+    b = g.vec()
+    g.kernel("init_b", b)
+    bh = g.get_vec(b)[: g.n]
+    bh[:, :3] += 1e-3 * np.random.default_rng(5).standard_normal((g.n, 3))
+    g.close()
+    whole = SlabSolve(maps_for(c), R.Ranks(1, 0, 0))
+    solves = [SlabSolve(maps_for(c), R.Ranks(world, r, r)) for r in range(world)]
+    try:
+        whole.load(bh)
+        ref = clean_div_local([whole], iters, thr)
+        b_ref = whole.owned(whole.b)
+        for s in solves:
+            s.load(bh)
+        got = clean_div_local(solves, iters, thr)
+        assert got["iterations"] == ref["iterations"] == iters
+        np.testing.assert_allclose(got["history"], ref["history"], rtol=1e-10)
+        assert ref["history"][-1] < 1e-2 * ref["history"][0]
+        scale = np.abs(bh[:, :3]).max()
+        for s in solves:
+            rows = s.slabs.global_rows()
+            assert np.abs(s.owned(s.b)[:, :3] - b_ref[rows, :3]).max() <= 1e-12 * scale
+        # B moved by the projection
+        assert np.abs(b_ref[:, :3] - bh[:, :3]).max() > 1e-6 * scale
+    finally:
+        whole.close()
+        for s in solves:
+            s.close()
+
+
+def test_dot_range_equals_dot_of_the_range():
+    # ieq_dot_range over a sub-range against the dot of the same elements; a range beyond the
+    # grid is refused
+    from inductioneq_b200.lib import IeqError
+    c = CASES["whistler_6c_hod_ck"]
+    ctx = maps_for(c).context()
+    rng = np.random.default_rng(9)
+    x, y = rng.standard_normal(ctx.n_pad), rng.standard_normal(ctx.n_pad)
+    dx, dy = ctx.scalar(x), ctx.scalar(y)
+    first, count = 1000, ctx.n - 3000
+    got = ctx.dot_range(dx, dy, first, count)
+    want = float(np.dot(x[first:first + count], y[first:first + count]))
+    assert abs(got - want) <= 1e-12 * abs(np.abs(x[first:first + count] * y[first:first + count]).sum())
+    assert ctx.dot_range(dx, dy, 0, ctx.n) == ctx.dot(dx, dy)
+    assert ctx.dot_range(dx, dy, 5, 0) == 0.0
+    with pytest.raises(IeqError):
+        ctx.dot_range(dx, dy, ctx.n - 10, 11)
+    ctx.close()
 
 
 def test_stage_api_refuses_misuse():
