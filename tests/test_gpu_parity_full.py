@@ -20,7 +20,8 @@ Configurations (synthetic inputs from the testcases, as the benchmark uses them)
 * rotation 40^3: [-1, 1]^3, 4th-order SBP, rigid rotation u = (-y, x, 0), Gaussian-bump B,
   SAT inflow, SSPRK33, dt = 1/56 (CFL 0.5);
 * whistler 64^3: [0, 2 pi]^3 periodic, 6th-order SBP + high-order dissipation, Hall, u = 0,
-  CarpenterKennedy2N54, dt = 0.5/260;
+  CarpenterKennedy2N54, dt = 0.5/260; the same at 144^3 (dt = 0.2 dx^2), where the curl kernel
+  is the pipelined 2.5D z march;
 * confined Hall 128^3: [0, 1]^3, 4th-order SBP, Hall with the testcase's velocity (and with
   u = 0), CarpenterKennedy2N54, dt = 0.2 dx^2; B + 1e-3 seeded uniform noise for the CG.
 """
@@ -121,6 +122,14 @@ def test_rotation_40_one_step_matches_reference():
 
 def test_whistler_64_one_step_matches_reference():
     _one_step_both_paths(C2)
+
+
+@pytest.mark.parametrize("curl_z", [None, 0])
+def test_whistler_144_one_step_matches_reference(curl_z):
+    # 144^3 = 2.99 M nodes: above 2^21 the launch policy (curl_z None: the default) takes the
+    # pipelined 2.5D curl kernel for this configuration; 0 forces the pair curl kernel
+    dx = TWO_PI / 144
+    _one_step_both_paths(dict(C2, nodes=(144, 144, 144), dt=0.2 * dx * dx, curl_z=curl_z))
 
 
 @pytest.mark.parametrize("real", ["double", "float"])
