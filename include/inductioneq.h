@@ -264,8 +264,9 @@ ieq_status ieq_stages_end(ieq_ctx *ctx, void *b, void *b2, void *b3, void *curlB
  * with J = curl(b)/rho, high-order and first-order dissipation, inflow SAT, Hall outflow SAT)
  * at fixed u and rho, and of the SSPRK33 and 2N steps.  No counterpart in the reference.
  * FP64 only.  The Hall outflow SAT switches on the sign of 0.5u - J: it is differentiated with
- * the switch held (its derivative away from tv = 0).  Adaptive dissipation (weights that depend
- * on b) returns IEQ_ERR_SETTINGS.  Vector fields in the reference layout. */
+ * the switch held (its derivative away from tv = 0).  Adaptive dissipation is linearised at b
+ * (kappa's derivative inside its thresholds; none exists at them).  Vector fields in the
+ * reference layout. */
 /* out = F'(b) v (tangent linear) */
 ieq_status ieq_operator_jvp(ieq_ctx *ctx, const void *b, const void *v, const void *u, const void *rho,
                             void *out);

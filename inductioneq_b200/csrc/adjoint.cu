@@ -31,6 +31,8 @@ struct AdjArgs {
   const Tables<double> *tab;
   int nb, sw, wh, periodic;
   int conv, hall, hod, fo;   // fo: first-order dissipation (linear in b at fixed u)
+  int ad;                    // adaptive dissipation (its weights depend on b: linearised at b0)
+  double mp2min, mp2max, cmin, cmax, hsgn;   // the adaptive form's thresholds; (-1)^(p/2+1)
   double hod_factor;
   double w[6];           // flux-form weights (see stage_kernel.cuh)
   double inv_d[3], two_inv_d[3], sat_s[3];
@@ -181,6 +183,191 @@ __device__ V3<double> fo_apply(const AdjArgs &a, const Node &nd, int ax, const R
   return s;
 }
 
+// Adaptive dissipation (artificial_dissipation.cl:82-160 with kappa of
+// include/artificial_dissipation.h:23-45), per component, along axis a with d = DX_a:
+//   first-order part  sum_o |D[row k][o]| kappa_|o|(s) sigma (b_{k+o} - b_k) / d,
+//   high-order part   sum_t hf (1 - kappa_1(s'_t)) sum_i c(row k, t, i) b_{k+t+i},
+// sigma = max(|u_j|, |u_k|) of the pair, s = (sigma delta) delta with delta the pair's
+// difference of b, and s'_t that of the pair (k+t+WH-1, k+t+WH-2).  kappa_m(s) is
+// sqrt(|s - lo| / |hi - lo|) on (lo, hi), 0 below, 1 above (lo, hi = m^2 MP2MIN CMIN d,
+// m^2 MP2MAX CMAX d); linearised at b0 its derivative is 1 / (2 |hi - lo| kappa) on (lo, hi)
+// and 0 elsewhere (it has none at s = lo and s = hi).  So along a pair, d(kappa sigma delta) =
+// sigma (kappa + 2 s kappa') d(delta), and d((1 - kappa_1(s')) H) = (1 - kappa_1) dH -
+// kappa_1' 2 sigma' delta' d(delta') H.
+struct KapLin {
+  double k, dk;
+};
+__device__ __forceinline__ KapLin kap_lin(const AdjArgs &a, unsigned m, double d, double s) {
+  m = m + (m == 0);
+  const double kk = (double)(m * m);
+  const double lo = ((kk * a.mp2min) * a.cmin) * d;
+  const double hi = ((kk * a.mp2max) * a.cmax) * d;
+  if (lo < s && s < hi) {
+    const double den = fabs(hi - lo);
+    const double k = sqrt(fabs(s - lo) / den);
+    return {k, k > 0.0 ? 0.5 / (den * k) : 0.0};
+  }
+  return {s >= hi ? 1.0 : 0.0, 0.0};
+}
+// sigma (kappa + 2 s kappa') of the pair (p, q) per component: the first-order part's
+// linearised weight (symmetric in the pair)
+__device__ __forceinline__ V3<double> ad_pair_weight(const AdjArgs &a, unsigned m, double d, V3<double> bp,
+                                                     V3<double> bq, V3<double> up, V3<double> uq) {
+  const V3<double> sg = sigma3(up, uq);
+  const double dl[3] = {bp.x - bq.x, bp.y - bq.y, bp.z - bq.z};
+  const double sgc[3] = {sg.x, sg.y, sg.z};
+  double w[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double sv = (sgc[c] * dl[c]) * dl[c];
+    const KapLin K = kap_lin(a, m, d, sv);
+    w[c] = sgc[c] * (K.k + 2.0 * sv * K.dk);
+  }
+  return {w[0], w[1], w[2]};
+}
+
+// the first-order part along ax (times 1/d by the caller): the tangent, or its transpose as
+// fo_apply<true> with the pair weights
+template <bool TR>
+__device__ V3<double> ad_fo_apply(const AdjArgs &a, const Node &nd, int ax, const R4<double> *x) {
+  const int c0 = (a.sw - 1) / 2;
+  const int rk = row_of(a, nd.i[ax], nd.n[ax]);
+  const double d = a.m.d[ax];
+  const V3<double> uk = ld(a.u, nd.idx), bk = ld(a.b0, nd.idx), xk = ld(x, nd.idx);
+  V3<double> s = {0, 0, 0}, diag = {0, 0, 0};
+  for (int o = -c0; o <= c0; ++o) {
+    long long j;
+    int jj;
+    if (!nbr_idx(a, nd, ax, o, j, jj)) continue;
+    const double cf = fabs(a.tab->D[rk][o + c0]);
+    const double ct = TR ? fabs(a.tab->D[row_of(a, jj, nd.n[ax])][c0 - o]) : 0.0;
+    if (cf == 0.0 && ct == 0.0) continue;
+    const V3<double> w = ad_pair_weight(a, (unsigned)(o < 0 ? -o : o), d, ld(a.b0, j), bk, ld(a.u, j), uk);
+    const V3<double> xj = ld(x, j);
+    if (!TR) {
+      s.x += cf * w.x * (xj.x - xk.x);
+      s.y += cf * w.y * (xj.y - xk.y);
+      s.z += cf * w.z * (xj.z - xk.z);
+    } else {
+      diag = {diag.x + cf * w.x, diag.y + cf * w.y, diag.z + cf * w.z};
+      s.x += ct * w.x * xj.x;
+      s.y += ct * w.y * xj.y;
+      s.z += ct * w.z * xj.z;
+    }
+  }
+  if (TR) s = {s.x - diag.x * xk.x, s.y - diag.y * xk.y, s.z - diag.z * xk.z};
+  return s;
+}
+
+// position of node + o along ax with the reference's neighbour rule: periodic wrap, or the
+// node itself outside a box (include/utils.h:89-168)
+__device__ __forceinline__ int ad_pos(const AdjArgs &a, int i, int o, int n) {
+  int t = i + o;
+  if (a.periodic) {
+    t += (t < 0) ? n : 0;
+    t -= (t >= n) ? n : 0;
+  } else if (t < 0 || t >= n) {
+    t = i;
+  }
+  return t;
+}
+
+// one high-order term t of node k (position ik along ax, grid index kidx): the pair weight
+// kappa_1 and its derivative factor 2 kappa_1' sigma' delta' per component, the pair's
+// positions, and the dissipation row applied to b0 (only where that factor is non-zero)
+struct AdTerm {
+  int p1, p2;
+  V3<double> one_minus_k, dfac, h0;
+};
+__device__ AdTerm ad_term(const AdjArgs &a, const Node &nd, int ax, int ik, long long kidx, int rk, int t) {
+  const int n = nd.n[ax];
+  const long long st = nd.st[ax];
+  AdTerm r;
+  r.p1 = ad_pos(a, ik, t + a.wh - 1, n);
+  r.p2 = ad_pos(a, ik, t + a.wh - 2, n);
+  const long long j1 = kidx + (long long)(r.p1 - ik) * st, j2 = kidx + (long long)(r.p2 - ik) * st;
+  const V3<double> b1 = ld(a.b0, j1), b2 = ld(a.b0, j2);
+  const V3<double> sg = sigma3(ld(a.u, j1), ld(a.u, j2));
+  const double dl[3] = {b1.x - b2.x, b1.y - b2.y, b1.z - b2.z}, sgc[3] = {sg.x, sg.y, sg.z};
+  double om[3], df[3];
+  bool any = false;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double sv = (sgc[c] * dl[c]) * dl[c];
+    const KapLin K = kap_lin(a, 1, a.m.d[ax], sv);
+    om[c] = 1.0 - K.k;
+    df[c] = 2.0 * K.dk * sgc[c] * dl[c];
+    any = any || df[c] != 0.0;
+  }
+  r.one_minus_k = {om[0], om[1], om[2]};
+  r.dfac = {df[0], df[1], df[2]};
+  r.h0 = {0, 0, 0};
+  if (any) {
+    for (int i = 0; i < a.wh; ++i) {
+      const double cf = ((a.tab->Minv[rk] * a.tab->DHO[rk][t + a.wh - 1]) * a.tab->DHO[a.nb][i]) * a.hsgn;
+      const int pi = ad_pos(a, ik, i + t, n);
+      r.h0 = axpy3(cf, ld(a.b0, kidx + (long long)(pi - ik) * st), r.h0);
+    }
+  }
+  return r;
+}
+
+// the high-order part along ax (times hod_factor by the caller): the tangent at the node, or
+// its transpose gathered from every node k whose terms reach the node (k within WH-1 along ax)
+template <bool TR>
+__device__ V3<double> ad_ho_apply(const AdjArgs &a, const Node &nd, int ax, const R4<double> *x) {
+  const int n = nd.n[ax], im = nd.i[ax];
+  const long long st = nd.st[ax];
+  V3<double> out = {0, 0, 0};
+  if (!TR) {
+    const int rk = row_of(a, im, n);
+    for (int t = -a.wh + 1; t <= 0; ++t) {
+      const AdTerm T = ad_term(a, nd, ax, im, nd.idx, rk, t);
+      V3<double> hv = {0, 0, 0};
+      for (int i = 0; i < a.wh; ++i) {
+        const double cf = ((a.tab->Minv[rk] * a.tab->DHO[rk][t + a.wh - 1]) * a.tab->DHO[a.nb][i]) * a.hsgn;
+        const int pi = ad_pos(a, im, i + t, n);
+        hv = axpy3(cf, ld(x, nd.idx + (long long)(pi - im) * st), hv);
+      }
+      const V3<double> x1 = ld(x, nd.idx + (long long)(T.p1 - im) * st), x2 = ld(x, nd.idx + (long long)(T.p2 - im) * st);
+      out.x += T.one_minus_k.x * hv.x - T.dfac.x * (x1.x - x2.x) * T.h0.x;
+      out.y += T.one_minus_k.y * hv.y - T.dfac.y * (x1.y - x2.y) * T.h0.y;
+      out.z += T.one_minus_k.z * hv.z - T.dfac.z * (x1.z - x2.z) * T.h0.z;
+    }
+    return out;
+  }
+  for (int off = -(a.wh - 1); off <= a.wh - 1; ++off) {
+    // node k = m + off along ax (a box has no node beyond its faces)
+    int ik = im + off;
+    if (a.periodic) {
+      ik += (ik < 0) ? n : 0;
+      ik -= (ik >= n) ? n : 0;
+    } else if (ik < 0 || ik >= n) {
+      continue;
+    }
+    const long long kidx = nd.idx + (long long)(ik - im) * st;
+    const int rk = row_of(a, ik, n);
+    const V3<double> wk = ld(x, kidx);
+    for (int t = -a.wh + 1; t <= 0; ++t) {
+      const AdTerm T = ad_term(a, nd, ax, ik, kidx, rk, t);
+      for (int i = 0; i < a.wh; ++i) {
+        if (ad_pos(a, ik, i + t, n) != im) continue;
+        const double cf = ((a.tab->Minv[rk] * a.tab->DHO[rk][t + a.wh - 1]) * a.tab->DHO[a.nb][i]) * a.hsgn;
+        out.x += T.one_minus_k.x * cf * wk.x;
+        out.y += T.one_minus_k.y * cf * wk.y;
+        out.z += T.one_minus_k.z * cf * wk.z;
+      }
+      const double sgn = (T.p1 == im ? -1.0 : 0.0) + (T.p2 == im ? 1.0 : 0.0);
+      if (sgn != 0.0) {
+        out.x += sgn * T.dfac.x * T.h0.x * wk.x;
+        out.y += sgn * T.dfac.y * T.h0.y * wk.y;
+        out.z += sgn * T.dfac.z * T.h0.z * wk.z;
+      }
+    }
+  }
+  return out;
+}
+
 // The Hall outflow SAT at a boundary node (induction_Eq_surface.cl:35-81), per face axis a
 // with c = M_INV[0]/d_a, tv = 0.5 u - J (J = curl(b)/rho), sw = -[left, tv_a > 0] + [right,
 // tv_a < 0], side = -[left] + [right]:  S = c (sw tv_a b + side b_a J).  Away from tv_a = 0
@@ -213,6 +400,7 @@ __device__ double sat_diag(const AdjArgs &a, const Node &nd, V3<double> um) {
 }
 
 // tangent linear F'(b0) v; dJ = curl(v)/rho precomputed
+template <bool AD>
 __global__ void k_jvp(const AdjArgs a) {
   Node nd;
   if (!make_node(a, nd)) return;
@@ -253,6 +441,10 @@ __global__ void k_jvp(const AdjArgs a) {
     }
     if (a.hod) out = axpy3(a.hod_factor, hod_apply<false>(a, nd, ax, a.v), out);
     if (a.fo) out = axpy3(a.inv_d[ax], fo_apply<false>(a, nd, ax, a.v), out);
+    if (AD) {
+      out = axpy3(a.inv_d[ax], ad_fo_apply<false>(a, nd, ax, a.v), out);
+      out = axpy3(a.hod_factor, ad_ho_apply<false>(a, nd, ax, a.v), out);
+    }
   }
   out = axpy3(sat_diag(a, nd, um), vm, out);
   if (a.hall && !a.periodic) {
@@ -347,7 +539,7 @@ __device__ __forceinline__ void vjp_store(const AdjArgs &a, long long k, V3<doub
 //   z_i += J0_a Q_a,i,  z_a -= J0 . Q_a,  and the source for dJ: gJ = sum_a (b0.Q_a) e_a - b0_a Q_a,
 // whose curl transpose (pass 2) adds C^T (gJ / rho).  On fast nodes the four gathers of an
 // axis share one pass over the neighbours (u and w loaded once per neighbour).
-template <int RI>
+template <int RI, bool AD = false>
 __global__ void k_vjp_pass1(const AdjArgs a) {
   Node nd;
   if (!make_node(a, nd)) return;
@@ -403,6 +595,10 @@ __global__ void k_vjp_pass1(const AdjArgs a) {
       pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
       if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
       if (a.fo) z = axpy3(a.inv_d[ax], fo_apply<true>(a, nd, ax, a.v), z);
+      if (AD) {
+        z = axpy3(a.inv_d[ax], ad_fo_apply<true>(a, nd, ax, a.v), z);
+        z = axpy3(a.hod_factor, ad_ho_apply<true>(a, nd, ax, a.v), z);
+      }
     }
   } else {
     if (a.hall) J0m = ld(a.J0, k);
@@ -425,6 +621,10 @@ __global__ void k_vjp_pass1(const AdjArgs a) {
       pass1_axis(a, ax, q, Du, S3, S5, wm, um, b0m, J0m, z, gJ);
       if (a.hod) z = axpy3(a.hod_factor, hod_apply<true>(a, nd, ax, a.v), z);
       if (a.fo) z = axpy3(a.inv_d[ax], fo_apply<true>(a, nd, ax, a.v), z);
+      if (AD) {
+        z = axpy3(a.inv_d[ax], ad_fo_apply<true>(a, nd, ax, a.v), z);
+        z = axpy3(a.hod_factor, ad_ho_apply<true>(a, nd, ax, a.v), z);
+      }
     }
   }
   z = axpy3(sat_diag(a, nd, um), wm, z);
@@ -523,6 +723,12 @@ AdjArgs adj_args(ieq_ctx *c) {
   a.hall = c->s.hall ? 1 : 0;
   a.hod = c->s.diss_form == 1 ? 1 : 0;
   a.fo = c->s.diss_form == 2 ? 1 : 0;
+  a.ad = c->s.diss_form == 3 ? 1 : 0;
+  a.mp2min = c->s.mp2min;
+  a.mp2max = c->s.mp2max;
+  a.cmin = c->s.cmin;
+  a.cmax = c->s.cmax;
+  a.hsgn = ((c->op.order / 2 + 1) % 2) ? -1.0 : 1.0;
   a.hod_factor = c->s.hod_factor;
   return a;
 }
@@ -537,8 +743,6 @@ ieq_status afail(ieq_ctx *c, ieq_status st, const std::string &m) {
 
 ieq_status check_adjoint_settings(ieq_ctx *c) {
   if (c->s.real_float) return afail(c, IEQ_ERR_SETTINGS, "the adjoint is FP64 only");
-  if (c->s.diss_form == 3)
-    return afail(c, IEQ_ERR_SETTINGS, "adaptive dissipation (weights that depend on b) has no adjoint");
   if (c->s.uibj < 0 || c->s.source < 0 || c->s.ujbi < 0) return afail(c, IEQ_ERR_SETTINGS, "no flux forms");
   return IEQ_OK;
 }
@@ -599,11 +803,15 @@ ieq_status vjp(ieq_ctx *c, const void *b, const void *w, const void *u, const vo
   a.rho = (const double *)rho;
   a.out = (R4<double> *)out;
   a.gJr = (R4<double> *)gJr;
-  if (c->s.hall && (!c->s.periodic || fast_ri(c) == 0)) {   // else pass 1 forms J0 at every node itself
+  // adaptive dissipation: its own instantiation of pass 1, generic rows on every node (the
+  // terms of its linearisation would raise the other instantiations' registers)
+  const int ri1 = a.ad ? 0 : fast_ri(c);
+  if (c->s.hall && (!c->s.periodic || ri1 == 0)) {   // else pass 1 forms J0 at every node itself
     adj_curl(c, b, rho, J0);
     a.J0 = (const R4<double> *)J0;
   }
-  switch (fast_ri(c)) {
+  switch (a.ad ? -1 : ri1) {
+    case -1: k_vjp_pass1<0, true><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
     case 1: k_vjp_pass1<1><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
     case 2: k_vjp_pass1<2><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
     case 3: k_vjp_pass1<3><<<agrid(c), ablock(), 0, c->stream>>>(a); break;
@@ -776,7 +984,8 @@ ieq_status ieq_operator_jvp(ieq_ctx *c, const void *b, const void *v, const void
     a.J0 = (const R4<double> *)w[0];
     a.dJ = (const R4<double> *)w[1];
   }
-  k_jvp<<<agrid(c), ablock(), 0, c->stream>>>(a);
+  if (a.ad) k_jvp<true><<<agrid(c), ablock(), 0, c->stream>>>(a);
+  else k_jvp<false><<<agrid(c), ablock(), 0, c->stream>>>(a);
   const cudaError_t e = cudaStreamSynchronize(c->stream);
   free_all(w);
   return e == cudaSuccess ? IEQ_OK : afail(c, IEQ_ERR_CUDA, cudaGetErrorString(e));

@@ -8,7 +8,7 @@
   (defined here, in the test harness only);
 * the same for the 2N low-storage schemes (CarpenterKennedy2N54, ToulorgeDesmet2N84F), for the
   2R schemes and SSPRK104 (the step's register program reversed), and for Hall on boxes (the
-  outflow SAT) and first-order dissipation.
+  outflow SAT) and first-order and adaptive dissipation.
 """
 from __future__ import annotations
 
@@ -42,6 +42,16 @@ CASES = {
     # first-order dissipation with convection only (its weights max(|u_j|, |u_k|) are fixed)
     "rot_2c_fo": dict(order=2, testcase="rotation_gaussian", nodes=(13, 12, 11), lo=-1.0, hi=1.0,
                       dissipation="FIRST_ORDER", integrator="SSPRK33"),
+    # adaptive dissipation: weights kappa(max|u| (b_j - b_k)^2) with a square root between two
+    # thresholds -- noise of amplitude 1 puts 40-50 % of the stencil pairs between them, the
+    # seeds keep every pair at least 1e-4 (relative) from a threshold, where kappa has no
+    # derivative
+    "rot_2c_ad": dict(order=2, testcase="rotation_gaussian", nodes=(13, 12, 11), lo=-1.0, hi=1.0,
+                      dissipation="ADAPTIVE", integrator="SSPRK33", noise=1.0, noise_seed=25),
+    # (with B noise of amplitude 1 the explicit Hall term needs a smaller step than 1e-3)
+    "confined_4c_hall_ad": dict(order=4, testcase="confined_domain", nodes=(15, 14, 13), lo=0.0, hi=1.0, hall=True,
+                                dissipation="ADAPTIVE", integrator="SSPRK33", noise=1.0, noise_seed=29,
+                                sweep_dt=1e-5),
 }
 
 
@@ -49,7 +59,7 @@ def _noisy(ctx, b, c):
     """B plus the case's seeded noise (off the outflow switch's non-smooth points)."""
     if c.get("noise"):
         bh = ctx.get_vec(b)
-        bh[: ctx.n, :3] += c["noise"] * np.random.default_rng(23).standard_normal((ctx.n, 3))
+        bh[: ctx.n, :3] += c["noise"] * np.random.default_rng(c.get("noise_seed", 23)).standard_normal((ctx.n, 3))
         b.upload(bh)
 
 
@@ -98,7 +108,8 @@ def ctx_nodes(ctx):
     return ctx._nodes
 
 
-@pytest.mark.parametrize("name", ["hallper_4c", "rot_6c_sat", "travel_6c_hall_box", "confined_4c_hall_fo", "rot_2c_fo"])
+@pytest.mark.parametrize("name", ["hallper_4c", "rot_6c_sat", "travel_6c_hall_box", "confined_4c_hall_fo", "rot_2c_fo",
+                                  "rot_2c_ad", "confined_4c_hall_ad"])
 def test_tangent_matches_central_differences(name):
     c = dict(CASES[name], integrator="CarpenterKennedy2N54")
     ctx, b, u, rho = _setup(c)
@@ -290,12 +301,13 @@ def test_low_storage_step_adjoint_matches_central_differences(integrator):
     ctx.close()
 
 
-@pytest.mark.parametrize("name", ["travel_6c_hall_box", "confined_4c_hall_fo"])
+@pytest.mark.parametrize("name", ["travel_6c_hall_box", "confined_4c_hall_fo", "rot_2c_ad", "confined_4c_hall_ad"])
 def test_sweep_through_hall_boxes_matches_central_differences(name):
     # the checkpointed SSPRK33 adjoint through steps with the Hall outflow SAT (and first-order
-    # dissipation) against Richardson-extrapolated central differences of the time stepping
+    # or adaptive dissipation) against Richardson-extrapolated central differences of the time
+    # stepping
     c = CASES[name]
-    ctx = maps_for(dict(c, dt=1e-3)).context()
+    ctx = maps_for(dict(c, dt=c.get("sweep_dt", 1e-3))).context()
     nsteps, every = 6, 4
     b, u = ctx.vec(), ctx.vec()
     ctx.kernel("init_b", b)
@@ -337,16 +349,6 @@ def test_sweep_through_hall_boxes_matches_central_differences(name):
         # somewhere along the trajectory, where the loss has a kink
         rich = (4.0 * cd(5e-7) - cd(1e-6)) / 3.0
         assert abs(rich - ad) <= 1e-6 * abs(ad), (k, rich, ad)
-    ctx.close()
-
-
-def test_adjoint_of_adaptive_dissipation_is_refused():
-    c = dict(CASES["rot_2c_fo"], dissipation="ADAPTIVE")
-    ctx = maps_for(dict(c, dt=1e-3)).context()
-    from inductioneq_b200.lib import IeqError
-    with pytest.raises(IeqError) as e:
-        ctx.operator_vjp(ctx.vec(), ctx.vec(), ctx.vec(), ctx.scalar(np.ones(ctx.n_pad)), ctx.vec())
-    assert e.value.name == "IEQ_ERR_SETTINGS"
     ctx.close()
 
 
