@@ -78,7 +78,28 @@ template <typename R>
 struct ColSums {
   V3<R> SuiBa, SU, SB, SuaB, SHo;
   R h1, h2;   // sum_k c_k E_c1(k), sum_k c_k E_c2(k) (see e_comp*)
+  V3<R> SFo;  // (FOF) sum_k (|c_k| max(|u_k|, |u_m|)) (B_k - B_m) of first-order dissipation
 };
+
+// one stencil point of the first-order dissipation of the axis (artificial_dissipation.cl
+// :36-78, the terms of fo_ad_dissipation in the same order): skipped where the derivative
+// coefficient is zero, as there
+template <typename R>
+__device__ __forceinline__ void fo_acc(ColSums<R> &s, R cD, const V3<R> &B, const V3<R> &U, const V3<R> &Bm,
+                                       const V3<R> &Um) {
+  const R cd = fabs(cD);
+  if (cd == (R)0) return;
+  s.SFo.x += (cd * fmax(fabs(U.x), fabs(Um.x))) * (B.x - Bm.x);
+  s.SFo.y += (cd * fmax(fabs(U.y), fabs(Um.y))) * (B.y - Bm.y);
+  s.SFo.z += (cd * fmax(fabs(U.z), fabs(Um.z))) * (B.z - Bm.z);
+}
+// the axis' first-order term into the node's sum: acc += tmp / DX (fo_ad_dissipation's order)
+template <typename R>
+__device__ __forceinline__ void fo_combine(const R *dR, int ax, const ColSums<R> &s, V3<R> &fo) {
+  fo.x += s.SFo.x / dR[ax];
+  fo.y += s.SFo.y / dR[ax];
+  fo.z += s.SFo.z / dR[ax];
+}
 
 // The two entries of E the Hall flux of axis ax needs, and their signs in DB:
 //   ax 0: DB_y += D[Exy], DB_z += D[Exz];  ax 1: DB_x -= D[Exy], DB_z += D[Eyz];
@@ -123,9 +144,12 @@ __device__ __forceinline__ void col_load(const StageArgs<R, F> &a, int ax, long 
 
 // the sums of one axis at one node (interior row, periodic wrap or SBP boundary row);
 // NEED >= 0 fixes the flux-form mask (StageArgs::need) at compile time
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, typename F = SoA<R>, int NEED = -1>
+// FOF: also the first-order dissipation terms of the axis (*Um: u at the node)
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, typename F = SoA<R>, int NEED = -1,
+          bool FOF = false>
 __device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, F> &a, int ax, int i, int n,
-                                         long long idx, long long st, const V3<R> &Bm) {
+                                         long long idx, long long st, const V3<R> &Bm,
+                                         const V3<R> *Um = nullptr) {
   const int need = NEED >= 0 ? NEED : a.need;
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
@@ -145,6 +169,7 @@ __device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, F> &a
       R e1 = 0, e2 = 0;
       col_load<R, HALL, HOD, CONV, F>(a, ax, j, B, U, e1, e2);
       col_acc<R, HALL, HOD, CONV>(s, ax, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B, U, e1, e2);
+      if (FOF) fo_acc(s, a.Dint[o + RI], B, U, Bm, *Um);
     }
   } else {
     for (int o = -RB; o <= RB; ++o) {
@@ -156,6 +181,7 @@ __device__ __forceinline__ void col_axis(ColSums<R> &s, const StageArgs<R, F> &a
       R e1 = 0, e2 = 0;
       col_load<R, HALL, HOD, CONV, F>(a, ax, j, B, U, e1, e2);
       col_acc<R, HALL, HOD, CONV>(s, ax, need, cD, cH, cD != (R)0, cH != (R)0, B, U, e1, e2);
+      if (FOF) fo_acc(s, cD, B, U, Bm, *Um);
     }
   }
 }

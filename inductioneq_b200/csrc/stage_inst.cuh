@@ -143,6 +143,20 @@ static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, in
   }
 }
 
+// the pair kernels with first-order dissipation summed in their gathers (FOF)
+template <bool H>
+static void launch_fo_pairs(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh, cudaStream_t s) {
+  if (banded(a, per, sh)) {
+    launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, H, false, 1, false, false, 10, true, true>,
+                  k_stage_xband<IEQ_R, IEQ_OP, H, false, 1, 10, false, false, true>, a, sh, s);
+    return;
+  }
+  const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
+  const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
+  if (per) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, H, false, 1, false, false, 10, false, true>, g2, b2, s, sh.pdl, a);
+  else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, H, false, 1, false, false, 10, false, true>, g2, b2, s, sh.pdl, a);
+}
+
 template <>
 void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hall, bool hod, int conv,
                                      bool hodp, bool foad, ColShape sh, cudaStream_t s) {
@@ -170,6 +184,19 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
       return;
     }
     launch_stage_hall_k<2>(a, per, hodp, sh, s);
+    return;
+  }
+  // convection (with or without the Hall term) + first-order dissipation with the default
+  // flux forms: two nodes per thread, the first-order terms summed in the gathers of the
+  // volume terms (FOF), which load the same B and u -- the one-node kernel gathers them a
+  // second time (measured on B200, CK2N54, 64^3, Hall: periodic with variable u 4th / 6th order
+  // 2.21e10 / 1.83e10 DOF/s against 1.12e10 / 8.2e9, confined box 1.80e10 / 1.30e10 against
+  // 1.17e10 / 7.4e9)
+  if (sh.pairs && conv && foad && a.diss_form == 2 && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
+      pair_ok(a.u) && pair_ok(a.E) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) &&
+      pair_ok(a.out2) && pair_ok(a.out3)) {
+    if (hall) launch_fo_pairs<true>(a, per, sh, s);
+    else launch_fo_pairs<false>(a, per, sh, s);
     return;
   }
   // Hall + convection with the default flux forms (the two convection sums per axis fixed

@@ -610,9 +610,9 @@ __device__ __forceinline__ void col_load_pair(const StageArgs<R, SoA<R>> &a, int
 }
 
 // the x sums of the pair (ix, ix + 1) on the interior row (or with periodic wrap)
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1, bool FOF = false>
 __device__ __forceinline__ void col_x_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, long long row0, int ix,
-                                           int nx) {
+                                           int nx, const V3<R> (*Bm)[2] = nullptr, const V3<R> (*Um)[2] = nullptr) {
   constexpr int RI = Op<OP>::RI, QL = (RI + 1) / 2;
   const int need = NEED >= 0 ? NEED : a.need;
   const V3<R> zero = {0, 0, 0};
@@ -639,15 +639,17 @@ __device__ __forceinline__ void col_x_pair(ColSums<R> (&s)[2], const StageArgs<R
         }
         col_acc<R, HALL, HOD, CONV>(s[k], 0, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B[e], U[e], e1[e],
                                     e2[e]);
+        if (FOF) fo_acc(s[k], a.Dint[o + RI], B[e], U[e], (*Bm)[k], (*Um)[k]);
       }
     }
   }
 }
 
 // the y or z sums of the pair (both nodes on the same row of the axis)
-template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1>
+template <typename R, int OP, bool PER, bool HALL, bool HOD, int CONV, int NEED = -1, bool FOF = false>
 __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<R, SoA<R>> &a, int ax, int i, int n,
-                                            long long idx, long long st, const V3<R> (&Bm)[2]) {
+                                            long long idx, long long st, const V3<R> (&Bm)[2],
+                                            const V3<R> (*Um)[2] = nullptr) {
   constexpr int NB = Op<OP>::NB, SW = Op<OP>::SW, C0 = (SW - 1) / 2, WH = Op<OP>::WH, RI = Op<OP>::RI;
   constexpr int RB = (C0 > WH - 1) ? C0 : WH - 1;
   const int need = NEED >= 0 ? NEED : a.need;
@@ -670,9 +672,11 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
       R e1[2] = {0, 0}, e2[2] = {0, 0};
       col_load_pair<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
+      for (int k = 0; k < 2; ++k) {
         col_acc<R, HALL, HOD, CONV>(s[k], ax, need, a.Dint[o + RI], a.Hint[o + RI], true, true, B[k], U[k], e1[k],
                                     e2[k]);
+        if (FOF) fo_acc(s[k], a.Dint[o + RI], B[k], U[k], Bm[k], (*Um)[k]);
+      }
     }
   } else {
     for (int o = -RB; o <= RB; ++o) {
@@ -684,8 +688,10 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
       R e1[2] = {0, 0}, e2[2] = {0, 0};
       col_load_pair<R, HALL, HOD, CONV>(a, ax, j, B, U, e1, e2);
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
+      for (int k = 0; k < 2; ++k) {
         col_acc<R, HALL, HOD, CONV>(s[k], ax, need, cD, cH, cD != (R)0, cH != (R)0, B[k], U[k], e1[k], e2[k]);
+        if (FOF) fo_acc(s[k], cD, B[k], U[k], Bm[k], (*Um)[k]);
+      }
     }
   }
 }
@@ -696,14 +702,30 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
 #ifndef IEQ_COL_X2_CONV_MIN_BLOCKS
 #define IEQ_COL_X2_CONV_MIN_BLOCKS 4
 #endif
+// resident blocks the pair kernel with fused first-order dissipation (FOF) is compiled for,
+// measured on B200 (Hall periodic 64^3 with variable u and the confined 64^3 box, CK2N54):
+// boxes 4 (4th / 6th order 1.80e10 / 1.30e10 DOF/s against 1.67e10 / 1.25e10 with 3), periodic
+// grids 3 at radius <= 2 (2.21e10 against 2.07e10 with 4 and 2.13e10 with 2) and 2 at radius 3
+// (1.83e10 against 1.59e10 with 3 and 1.34e10 with 4): the periodic x window of a pair is
+// loaded whole, and at radius 3 the first-order sums of both nodes spilled below 255 registers
+#ifndef IEQ_COL_X2_FO_MIN_BLOCKS
+#define IEQ_COL_X2_FO_MIN_BLOCKS 4
+#endif
+template <int OP, bool PER>
+__host__ __device__ constexpr int fo_min_blocks() {
+  return PER ? (Op<OP>::RI >= 3 ? 2 : 3) : IEQ_COL_X2_FO_MIN_BLOCKS;
+}
 
 // DB (volume, Hall, SAT, dissipation) and the stage update at the pair; template
 // arguments as k_stage_col (CONV = 1: the convection sums; HODP: the dissipation sum read
-// from a.Hpre; FOAD: first-order / adaptive dissipation)
+// from a.Hpre; FOAD: first-order / adaptive dissipation; FOF: first-order dissipation with
+// its terms summed in the gathers of the volume terms, which load the same B and u)
 template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false,
-          int NEED = -1, bool XBAND = false>
-__global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS)
+          int NEED = -1, bool XBAND = false, bool FOF = false>
+__global__ void __launch_bounds__(kColThreads, FOF ? fo_min_blocks<OP, PER>()
+                                                   : (CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS))
     k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
+  static_assert(!FOF || (CONV && !FOAD), "the fused first-order terms need the convection loads");
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel
   constexpr int X0 = XBAND ? xband<OP>() : 0;
   pdl_enter();
@@ -715,29 +737,35 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
     const long long row0 = (long long)nx * (iy + (long long)ny * iz);
     const long long idx = row0 + ix;
     const V3<R> zero = {0, 0, 0};
-    V3<R> Bm[2], um[2] = {zero, zero}, db[2] = {zero, zero}, hod[2] = {zero, zero};
+    V3<R> Bm[2], um[2] = {zero, zero}, db[2] = {zero, zero}, hod[2] = {zero, zero}, fo[2] = {zero, zero};
     ldf_pair(a.bk, idx, Bm[0], Bm[1]);
     if (CONV) ldf_pair(a.u, idx, um[0], um[1]);
     {
       ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
       if (XBAND || x_pair_interior<OP, PER>(ix, nx)) {
-        col_x_pair<R, OP, PER, HALL, HOD, CONV, NEED>(s, a, row0, ix, nx);
+        col_x_pair<R, OP, PER, HALL, HOD, CONV, NEED, FOF>(s, a, row0, ix, nx, &Bm, &um);
       } else {
 #pragma unroll
         for (int k = 0; k < 2; ++k)
-          col_axis<R, OP, PER, HALL, HOD, CONV, SoA<R>, NEED>(s[k], a, 0, ix + k, nx, idx + k, 1, Bm[k]);
+          col_axis<R, OP, PER, HALL, HOD, CONV, SoA<R>, NEED, FOF>(s[k], a, 0, ix + k, nx, idx + k, 1, Bm[k], &um[k]);
       }
 #pragma unroll
-      for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, 0, s[k], Bm[k], um[k], db[k], hod[k]);
+      for (int k = 0; k < 2; ++k) {
+        col_combine<R, HALL, HOD, CONV>(a, 0, s[k], Bm[k], um[k], db[k], hod[k]);
+        if (FOF) fo_combine(a.dR, 0, s[k], fo[k]);
+      }
     }
     const int nn[3] = {nx, ny, nz};
     const long long st[3] = {1, nx, (long long)nx * ny};
 #pragma unroll
     for (int ax = 1; ax < 3; ++ax) {
       ColSums<R> s[2] = {ColSums<R>{}, ColSums<R>{}};
-      col_yz_pair<R, OP, PER, HALL, HOD, CONV, NEED>(s, a, ax, ax == 1 ? iy : iz, nn[ax], idx, st[ax], Bm);
+      col_yz_pair<R, OP, PER, HALL, HOD, CONV, NEED, FOF>(s, a, ax, ax == 1 ? iy : iz, nn[ax], idx, st[ax], Bm, &um);
 #pragma unroll
-      for (int k = 0; k < 2; ++k) col_combine<R, HALL, HOD, CONV>(a, ax, s[k], Bm[k], um[k], db[k], hod[k]);
+      for (int k = 0; k < 2; ++k) {
+        col_combine<R, HALL, HOD, CONV>(a, ax, s[k], Bm[k], um[k], db[k], hod[k]);
+        if (FOF) fo_combine(a.dR, ax, s[k], fo[k]);
+      }
     }
     V3<R> hv[2] = {hod[0], hod[1]};
     if (HODP) ldf_pair(a.Hpre, idx, hv[0], hv[1]);
@@ -754,6 +782,9 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
         const V3<R> ds = fo_ad_dissipation<R, SoA<R>, OP, PER>(a, ii, nn, st, idx + k, Bm[k], um[k]);
         db[k].x += ds.x; db[k].y += ds.y; db[k].z += ds.z;
       }
+      if (FOF) {
+        db[k].x += fo[k].x; db[k].y += fo[k].y; db[k].z += fo[k].z;
+      }
     }
     stage_epilogue_pair(a, idx, db[0], db[1]);
   }
@@ -761,7 +792,7 @@ __global__ void __launch_bounds__(kColThreads, CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS
 }
 
 // One node of a box's stage in the order of operations of k_stage_col (one node per thread)
-template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD>
+template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD, bool FOF = false>
 __device__ __forceinline__ void col_stage_node(const StageArgs<R, SoA<R>> &a, int ix, int iy, int iz) {
   constexpr bool HOD = HOD_ && !HODP;
   const int nx = a.m.nx, ny = a.m.ny, nz = a.m.nz;
@@ -772,12 +803,13 @@ __device__ __forceinline__ void col_stage_node(const StageArgs<R, SoA<R>> &a, in
   const V3<R> zero = {0, 0, 0};
   const V3<R> Bm = ldf(a.bk, idx);
   const V3<R> um = CONV ? ldf(a.u, idx) : zero;
-  V3<R> db = zero, hod = zero;
+  V3<R> db = zero, hod = zero, fo = zero;
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
     ColSums<R> s{};
-    col_axis<R, OP, false, HALL, HOD, CONV, SoA<R>, NEED>(s, a, ax, ii[ax], nn[ax], idx, st[ax], Bm);
+    col_axis<R, OP, false, HALL, HOD, CONV, SoA<R>, NEED, FOF>(s, a, ax, ii[ax], nn[ax], idx, st[ax], Bm, &um);
     col_combine<R, HALL, HOD, CONV>(a, ax, s, Bm, um, db, hod);
+    if (FOF) fo_combine(a.dR, ax, s, fo);
   }
   stage_sat<R, SoA<R>, HALL>(a, ii, nn, idx, Bm, um, CONV, db);
   if (HOD_) {
@@ -790,12 +822,15 @@ __device__ __forceinline__ void col_stage_node(const StageArgs<R, SoA<R>> &a, in
     const V3<R> ds = fo_ad_dissipation<R, SoA<R>, OP, false>(a, ii, nn, st, idx, Bm, um);
     db.x += ds.x; db.y += ds.y; db.z += ds.z;
   }
+  if (FOF) {
+    db.x += fo.x; db.y += fo.y; db.z += fo.z;
+  }
   stage_epilogue<R, SoA<R>>(a, idx, db);
 }
 
 // the x boundary columns of a box (2 * xband nodes per row, one per thread), and the stage's
 // time bookkeeping
-template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD>
+template <typename R, int OP, bool HALL, bool HOD_, int CONV, int NEED, bool HODP, bool FOAD, bool FOF = false>
 __global__ void __launch_bounds__(kColThreads) k_stage_xband(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   constexpr int XB = xband<OP>();
   pdl_enter();
@@ -805,7 +840,7 @@ __global__ void __launch_bounds__(kColThreads) k_stage_xband(const __grid_consta
     const int slot = (int)(i % (2 * XB));
     const long long row = i / (2 * XB);
     const int ix = slot < XB ? slot : a.m.nx - 2 * XB + slot;
-    col_stage_node<R, OP, HALL, HOD_, CONV, NEED, HODP, FOAD>(a, ix, (int)(row % a.m.ny), (int)(row / a.m.ny));
+    col_stage_node<R, OP, HALL, HOD_, CONV, NEED, HODP, FOAD, FOF>(a, ix, (int)(row % a.m.ny), (int)(row / a.m.ny));
   }
   stage_time_post(a);
 }

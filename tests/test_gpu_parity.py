@@ -242,6 +242,23 @@ HALL_CONV_CASES = {
                                          dt=1e-3, steps=2),
     "confined_2c_hall_conv_box_f32": dict(order=2, testcase="confined_domain", nodes=(14, 12, 10), lo=0.0, hi=1.0,
                                           hall=True, integrator="SSPRK33", dt=1e-5, steps=2, real="float"),
+    # first-order dissipation summed in the pair kernels' gathers: a box (x boundary pairs per
+    # node), the same box with its x boundary columns in a launch of their own, a periodic grid
+    "confined_4c_hall_conv_fo_box": dict(order=4, testcase="confined_domain", nodes=(16, 13, 14), lo=0.0, hi=1.0,
+                                         hall=True, dissipation="FIRST_ORDER", integrator="CarpenterKennedy2N54",
+                                         dt=1e-5, steps=2),
+    "confined_6c_hall_conv_fo_band": dict(order=6, testcase="confined_domain", nodes=(20, 13, 14), lo=0.0, hi=1.0,
+                                          hall=True, dissipation="FIRST_ORDER", integrator="SSPRK33", dt=1e-5,
+                                          steps=2, xband=2),
+    "hallper_6c_hall_conv_fo_per": dict(order=6, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0, hi=HP_,
+                                        periodic=True, hall=True, dissipation="FIRST_ORDER", integrator="SSPRK33",
+                                        dt=1e-3, steps=2),
+    # the same without the Hall term (convection and first-order dissipation only)
+    "rotation_4c_conv_fo_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                    dissipation="FIRST_ORDER", integrator="SSPRK33", dt=0.01, steps=2),
+    "rotation_6c_conv_fo_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
+                                     dissipation="FIRST_ORDER", integrator="CarpenterKennedy2N54", dt=0.01, steps=2,
+                                     xband=2),
 }
 
 
@@ -263,12 +280,13 @@ def test_fused_hall_convection_pairs_match_oracle(name):
             np.zeros(2, dtype=o.T)]
     dev = [ctx.vec(host[0]), ctx.vec(), ctx.vec(), ctx.vec(), ctx.vec(u), ctx.scalar(host[5]),
            ctx.scalar(host[6], n=2)]
-    time_loop(o, c["integrator"], True, False, c["steps"], host[0], host[1], host[2] if nf == 3 else None,
+    hall = c.get("hall", False)
+    time_loop(o, c["integrator"], hall, False, c["steps"], host[0], host[1], host[2] if nf == 3 else None,
               host[3], host[4], host[5], host[6])
     ctx.time_steps(*dev, c["steps"])
     mb, mu = float(np.abs(host[0]).max()), float(np.abs(u).max())
     ns = stages_of(c, c["steps"])
-    for i in (0, 1, 3):
+    for i in (0, 1, 3) if hall else (0, 1):
         fl = {1: rounding_floor(c, "register", mb, mu, ns), 3: rounding_floor(c, "curl", mb, mu, ns)}.get(i, 0.0)
         ok, e = field_ok(ctx.get_vec(dev[i]), host[i], tol(c), fl)
         assert ok, (i, e)
@@ -625,7 +643,8 @@ def test_column_block_shape_does_not_change_the_result(shape, case):
 
 
 @pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32", "periodic_conv_hod",
-                                  "periodic_fo", "periodic_adaptive_conv", "rotation_o2", "rotation_o4",
+                                  "periodic_fo", "periodic_conv_fo", "box_conv_fo", "periodic_adaptive_conv",
+                                  "rotation_o2", "rotation_o4", "rotation_o4_fo", "rotation_o6_fo",
                                   "rotation_o6_f32", "quads_periodic_hod_f32", "quads_box_hod_f32",
                                   "quads_periodic_plain_f32"])
 def test_two_nodes_per_thread_equal_one_node_per_thread(case):
@@ -659,6 +678,8 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
     if case.startswith("rotation"):   # convection only, default flux forms, inflow SAT
         c = dict(order=int(case[10]), testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                  integrator="SSPRK33", dt=0.01, real="float" if case.endswith("f32") else "double")
+        if case.endswith("fo"):
+            c.update(dissipation="FIRST_ORDER")
     out = []
     for pairs in (0, 4 if case.startswith("quads") else 1):
         ctx = maps_for(dict(c, col_pairs=pairs)).context()
