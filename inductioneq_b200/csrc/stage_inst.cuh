@@ -100,12 +100,16 @@ static void launch_banded(KI kint, KB kband, const StageArgs<IEQ_R, SoA<IEQ_R>> 
   launch_pdl(kband, dim3((unsigned)((nb + kColThreads - 1) / kColThreads)), dim3(kColThreads), s, sh.pdl, a);
 }
 // whether a box's stage splits off its x boundary columns: even rows in which the band is at
-// most a tenth of the row (measured on B200: rotation 2nd order 96^3 +10 %, 6th order 128^3
-// +23 %, confined Hall 4th order 128^3 +12 % FP64 / +20 % FP32; 4th order 64^3, a band of
-// 8 of 64 columns, 14 % slower)
+// most a tenth of the row, and for a band of two columns a side (2nd order) rows of at least
+// 96 (measured on B200: rotation 2nd order 96^3 +10 %, 6th order 128^3 +23 %, confined Hall
+// 4th order 128^3 +12 % FP64 / +20 % FP32; 4th order 64^3, a band of 8 of 64 columns, 14 %
+// slower; rotation, SSPRK33, 40 steps: 2nd order banded 5-43 % slower at 40^3 .. 80^3 and 12 %
+// faster at 96^3 -- its one boundary row a side costs the pair kernel little, the band's
+// launch more -- 4th order banded faster from 80^3 (+8 %), 6th order from 120^3 (+29 %))
+inline int band_min_nx(int xb) { return xb <= 2 ? 96 : 20 * xb; }
 static bool banded(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh) {
   if (per || sh.band == 0 || a.m.nx % 2 != 0 || a.m.nx < 2 * xband<IEQ_OP>() + 2) return false;
-  return sh.band == 2 || a.m.nx >= 20 * xband<IEQ_OP>();
+  return sh.band == 2 || a.m.nx >= band_min_nx(xband<IEQ_OP>());
 }
 
 // the Hall stage kernel without convection, K x-adjacent nodes per thread
