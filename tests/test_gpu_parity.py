@@ -247,6 +247,9 @@ HALL_CONV_CASES = {
     "confined_4c_hall_conv_fo_box": dict(order=4, testcase="confined_domain", nodes=(16, 13, 14), lo=0.0, hi=1.0,
                                          hall=True, dissipation="FIRST_ORDER", integrator="CarpenterKennedy2N54",
                                          dt=1e-5, steps=2),
+    "confined_4c_hall_conv_fo_box_f32": dict(order=4, testcase="confined_domain", nodes=(16, 13, 14), lo=0.0,
+                                             hi=1.0, hall=True, dissipation="FIRST_ORDER", integrator="SSPRK33",
+                                             dt=1e-5, steps=2, real="float"),
     "confined_6c_hall_conv_fo_band": dict(order=6, testcase="confined_domain", nodes=(20, 13, 14), lo=0.0, hi=1.0,
                                           hall=True, dissipation="FIRST_ORDER", integrator="SSPRK33", dt=1e-5,
                                           steps=2, xband=2),
@@ -643,7 +646,8 @@ def test_column_block_shape_does_not_change_the_result(shape, case):
 
 
 @pytest.mark.parametrize("case", ["periodic_hod", "box_hod", "box_plain", "periodic_plain_f32", "periodic_conv_hod",
-                                  "periodic_fo", "periodic_conv_fo", "box_conv_fo", "periodic_adaptive_conv",
+                                  "periodic_fo", "periodic_conv_fo", "box_conv_fo", "box_conv_fo_f32",
+                                  "periodic_adaptive_conv",
                                   "rotation_o2", "rotation_o4", "rotation_o4_fo", "rotation_o6_fo",
                                   "rotation_o6_f32", "quads_periodic_hod_f32", "quads_box_hod_f32",
                                   "quads_periodic_plain_f32"])
@@ -663,7 +667,7 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
         c.update(testcase="hall_travelling_wave")
     if "conv" in case:   # variable velocity: the convection sums beside the Hall term
         c.update(testcase="hall_periodic", hi=HP_, variable_u=True, dt=1e-3)
-    if case.endswith("fo"):
+    if case.endswith("fo") or "_fo_" in case:
         c.update(dissipation="FIRST_ORDER")
     if case.startswith("periodic_adaptive"):
         c.update(dissipation="ADAPTIVE")
