@@ -147,6 +147,20 @@ static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, in
   }
 }
 
+// the convection pair kernels (no Hall term, no dissipation) with the flux-form mask N
+template <int N>
+static void launch_conv_pairs(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh, cudaStream_t s) {
+  if (banded(a, per, sh)) {
+    launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, N, true>,
+                  k_stage_xband<IEQ_R, IEQ_OP, false, false, 1, N, false, false>, a, sh, s);
+    return;
+  }
+  const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
+  const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
+  if (per) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, false, false, 1, false, false, N>, g2, b2, s, sh.pdl, a);
+  else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, N>, g2, b2, s, sh.pdl, a);
+}
+
 // the pair kernels with first-order dissipation summed in their gathers (FOF)
 template <bool H>
 static void launch_fo_pairs(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh, cudaStream_t s) {
@@ -247,19 +261,16 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   // convection without the Hall term, with the reference's default flux forms (product
   // u_i B_j, central source and u_j B_i: the sums D[u] and D[u_a B_i] only, fixed at compile
   // time, which keeps two nodes' sums in 128 registers): measured 2-10 % faster than one node
-  // per thread (rotation, orders 2/4/6, 64^3 .. 128^3); other forms keep one node per thread
-  if (sh.pairs && !hall && conv && !hod && !foad && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
-      pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) &&
-      pair_ok(a.out3)) {
-    if (banded(a, per, sh)) {
-      launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, 10, true>,
-                    k_stage_xband<IEQ_R, IEQ_OP, false, false, 1, 10, false, false>, a, sh, s);
-      return;
-    }
-    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
-    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
-    if (per) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, false, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
-    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, false, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
+  // per thread (rotation, orders 2/4/6, 64^3 .. 128^3).  The two other forms of two sums per
+  // axis take the same kernel with their own mask (central u_i B_j and u_j B_i with zero
+  // source: D[u_i B_a], D[u_a B_i], mask 9; product u_i B_j and u_j B_i with central source:
+  // D[u], D[B], mask 6); forms of three or four sums keep one node per thread
+  if (sh.pairs && !hall && conv && !hod && !foad && (a.need == 10 || a.need == 9 || a.need == 6) &&
+      a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) &&
+      pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
+    if (a.need == 9) launch_conv_pairs<9>(a, per, sh, s);
+    else if (a.need == 6) launch_conv_pairs<6>(a, per, sh, s);
+    else launch_conv_pairs<10>(a, per, sh, s);
     return;
   }
   if (per) {

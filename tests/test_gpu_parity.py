@@ -259,6 +259,16 @@ HALL_CONV_CASES = {
     # the same without the Hall term (convection and first-order dissipation only)
     "rotation_4c_conv_fo_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                                     dissipation="FIRST_ORDER", integrator="SSPRK33", dt=0.01, steps=2),
+    # convection only with the two other flux forms of two sums per axis (masks 9 and 6)
+    "rotation_4c_czc_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                uibj="CENTRAL", source="ZERO", ujbi="CENTRAL", integrator="SSPRK33", dt=0.01,
+                                steps=2),
+    "rotation_6c_pcp_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
+                                 uibj="PRODUCT", source="CENTRAL", ujbi="PRODUCT", integrator="CarpenterKennedy2N54",
+                                 dt=0.01, steps=2, xband=2),
+    "rotation_2c_pcp_per": dict(order=2, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                periodic=True, uibj="PRODUCT", source="CENTRAL", ujbi="PRODUCT", integrator="SSPRK33",
+                                dt=0.01, steps=2),
     "rotation_6c_conv_fo_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
                                      dissipation="FIRST_ORDER", integrator="CarpenterKennedy2N54", dt=0.01, steps=2,
                                      xband=2),
@@ -649,6 +659,7 @@ def test_column_block_shape_does_not_change_the_result(shape, case):
                                   "periodic_fo", "periodic_conv_fo", "box_conv_fo", "box_conv_fo_f32",
                                   "periodic_adaptive_conv",
                                   "rotation_o2", "rotation_o4", "rotation_o4_fo", "rotation_o6_fo",
+                                  "rotation_o4_czc", "rotation_o6_pcp",
                                   "rotation_o6_f32", "quads_periodic_hod_f32", "quads_box_hod_f32",
                                   "quads_periodic_plain_f32"])
 def test_two_nodes_per_thread_equal_one_node_per_thread(case):
@@ -684,6 +695,10 @@ def test_two_nodes_per_thread_equal_one_node_per_thread(case):
                  integrator="SSPRK33", dt=0.01, real="float" if case.endswith("f32") else "double")
         if case.endswith("fo"):
             c.update(dissipation="FIRST_ORDER")
+        if case.endswith("czc"):
+            c.update(uibj="CENTRAL", source="ZERO", ujbi="CENTRAL")
+        if case.endswith("pcp"):
+            c.update(uibj="PRODUCT", source="CENTRAL", ujbi="PRODUCT")
     out = []
     for pairs in (0, 4 if case.startswith("quads") else 1):
         ctx = maps_for(dict(c, col_pairs=pairs)).context()
