@@ -261,16 +261,23 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   // convection without the Hall term, with the reference's default flux forms (product
   // u_i B_j, central source and u_j B_i: the sums D[u] and D[u_a B_i] only, fixed at compile
   // time, which keeps two nodes' sums in 128 registers): measured 2-10 % faster than one node
-  // per thread (rotation, orders 2/4/6, 64^3 .. 128^3).  The two other forms of two sums per
-  // axis take the same kernel with their own mask (central u_i B_j and u_j B_i with zero
-  // source: D[u_i B_a], D[u_a B_i], mask 9; product u_i B_j and u_j B_i with central source:
-  // D[u], D[B], mask 6); forms of three or four sums keep one node per thread
-  if (sh.pairs && !hall && conv && !hod && !foad && (a.need == 10 || a.need == 9 || a.need == 6) &&
+  // per thread (rotation, orders 2/4/6, 64^3 .. 128^3).  Every other mask of the split forms
+  // takes the same kernel with its own mask compiled in (two sums per axis: central u_i B_j
+  // and u_j B_i with zero source, mask 9; product u_i B_j and u_j B_i with central source,
+  // mask 6; three or four sums, masks 13, 14, 15, at 3 blocks of <= 168 registers): measured
+  // 1.06-1.43x faster than one node per thread at 80^3 and 160^3 (rotation 3D, orders 2/4/6)
+  if (sh.pairs && !hall && conv && !hod && !foad &&
+      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 13 || a.need == 14 || a.need == 15) &&
       a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) &&
       pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
-    if (a.need == 9) launch_conv_pairs<9>(a, per, sh, s);
-    else if (a.need == 6) launch_conv_pairs<6>(a, per, sh, s);
-    else launch_conv_pairs<10>(a, per, sh, s);
+    switch (a.need) {
+      case 9: launch_conv_pairs<9>(a, per, sh, s); break;
+      case 6: launch_conv_pairs<6>(a, per, sh, s); break;
+      case 13: launch_conv_pairs<13>(a, per, sh, s); break;
+      case 14: launch_conv_pairs<14>(a, per, sh, s); break;
+      case 15: launch_conv_pairs<15>(a, per, sh, s); break;
+      default: launch_conv_pairs<10>(a, per, sh, s); break;
+    }
     return;
   }
   if (per) {

@@ -711,6 +711,14 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
 #ifndef IEQ_COL_X2_FO_MIN_BLOCKS
 #define IEQ_COL_X2_FO_MIN_BLOCKS 4
 #endif
+// resident blocks of the convection pair kernel with a compile-time flux-form mask: masks of
+// three or four sums per axis (13, 14, 15) get more registers (3 blocks of <= 168)
+template <int NEED>
+__host__ __device__ constexpr int conv_min_blocks() {
+  return (NEED >= 0 && ((NEED & 1) + ((NEED >> 1) & 1) + ((NEED >> 2) & 1) + ((NEED >> 3) & 1)) >= 3)
+             ? 3
+             : IEQ_COL_X2_CONV_MIN_BLOCKS;
+}
 template <int OP, bool PER>
 __host__ __device__ constexpr int fo_min_blocks() {
   return PER ? (Op<OP>::RI >= 3 ? 2 : 3) : IEQ_COL_X2_FO_MIN_BLOCKS;
@@ -723,7 +731,7 @@ __host__ __device__ constexpr int fo_min_blocks() {
 template <typename R, int OP, bool PER, bool HALL, bool HOD_, int CONV, bool HODP = false, bool FOAD = false,
           int NEED = -1, bool XBAND = false, bool FOF = false>
 __global__ void __launch_bounds__(kColThreads, FOF ? fo_min_blocks<OP, PER>()
-                                                   : (CONV ? IEQ_COL_X2_CONV_MIN_BLOCKS : IEQ_COL_X2_MIN_BLOCKS))
+                                                   : (CONV ? conv_min_blocks<NEED>() : IEQ_COL_X2_MIN_BLOCKS))
     k_stage_col_x2(const __grid_constant__ StageArgs<R, SoA<R>> a) {
   static_assert(!FOF || (CONV && !FOAD), "the fused first-order terms need the convection loads");
   constexpr bool HOD = HOD_ && !HODP;   // the dissipation rows gathered in this kernel

@@ -269,6 +269,14 @@ HALL_CONV_CASES = {
     "rotation_2c_pcp_per": dict(order=2, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                                 periodic=True, uibj="PRODUCT", source="CENTRAL", ujbi="PRODUCT", integrator="SSPRK33",
                                 dt=0.01, steps=2),
+    "rotation_4c_ccc_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                uibj="CENTRAL", source="CENTRAL", ujbi="CENTRAL", integrator="SSPRK33", dt=0.01,
+                                steps=2),
+    "rotation_6c_pcs_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
+                                 uibj="PRODUCT", source="CENTRAL", ujbi="SPLIT", integrator="SSPRK33", dt=0.01,
+                                 steps=2, xband=2),
+    "rotation_2c_scs_box": dict(order=2, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                uibj="SPLIT", source="CENTRAL", ujbi="SPLIT", integrator="SSPRK33", dt=0.01, steps=2),
     "rotation_6c_conv_fo_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
                                      dissipation="FIRST_ORDER", integrator="CarpenterKennedy2N54", dt=0.01, steps=2,
                                      xband=2),
