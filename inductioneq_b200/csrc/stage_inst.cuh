@@ -147,6 +147,31 @@ static void launch_col_x2_ph(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool hod, in
   }
 }
 
+// the Hall + convection pair kernels with the flux-form mask N (high-order dissipation, if
+// any, precomputed by the curl kernel: HODP)
+template <int N>
+static void launch_hall_conv_pairs(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, bool hodp, ColShape sh,
+                                   cudaStream_t s) {
+  if (banded(a, per, sh)) {
+    if (hodp)
+      launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, true, 1, true, false, N, true>,
+                    k_stage_xband<IEQ_R, IEQ_OP, true, true, 1, N, true, false>, a, sh, s);
+    else
+      launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, false, 1, false, false, N, true>,
+                    k_stage_xband<IEQ_R, IEQ_OP, true, false, 1, N, false, false>, a, sh, s);
+    return;
+  }
+  const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
+  const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
+  if (per) {
+    if (hodp) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, true, true, 1, true, false, N>, g2, b2, s, sh.pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, true, false, 1, false, false, N>, g2, b2, s, sh.pdl, a);
+  } else {
+    if (hodp) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, true, 1, true, false, N>, g2, b2, s, sh.pdl, a);
+    else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, false, 1, false, false, N>, g2, b2, s, sh.pdl, a);
+  }
+}
+
 // the convection pair kernels (no Hall term, no dissipation) with the flux-form mask N
 template <int N>
 static void launch_conv_pairs(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool per, ColShape sh, cudaStream_t s) {
@@ -217,30 +242,22 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
     else launch_fo_pairs<false>(a, per, sh, s);
     return;
   }
-  // Hall + convection with the default flux forms (the two convection sums per axis fixed
-  // at compile time): two nodes per thread on every grid -- measured 24-27 % faster on
-  // periodic grids than the run-time-masked pair kernel below and 6 % faster than one node
-  // per thread on boxes (confined Hall 128^3)
-  if (sh.pairs && hall && conv && !foad && (hodp || !hod) && a.need == 10 && a.m.nx % 2 == 0 && pair_ok(a.bk) &&
-      pair_ok(a.u) && pair_ok(a.E) && pair_ok(a.Hpre) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) &&
-      pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
-    if (banded(a, per, sh)) {
-      if (hodp)
-        launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, true, 1, true, false, 10, true>,
-                      k_stage_xband<IEQ_R, IEQ_OP, true, true, 1, 10, true, false>, a, sh, s);
-      else
-        launch_banded(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, false, 1, false, false, 10, true>,
-                      k_stage_xband<IEQ_R, IEQ_OP, true, false, 1, 10, false, false>, a, sh, s);
-      return;
-    }
-    const ColShape ps = pair_shape(sh, false, (long long)a.m.nx * a.m.ny * a.m.nz, a.m.nx);
-    const dim3 g2 = col_grid(ps, a.m.nx / 2, a.m.ny, a.m.nz, 1), b2 = col_block(ps);
-    if (per) {
-      if (hodp) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, true, true, 1, true, false, 10>, g2, b2, s, sh.pdl, a);
-      else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, true, true, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
-    } else {
-      if (hodp) launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, true, 1, true, false, 10>, g2, b2, s, sh.pdl, a);
-      else launch_pdl(k_stage_col_x2<IEQ_R, IEQ_OP, false, true, false, 1, false, false, 10>, g2, b2, s, sh.pdl, a);
+  // Hall + convection with the flux-form mask compiled in (the default forms' two
+  // convection sums per axis, mask 10, and every other mask of the split forms): two nodes
+  // per thread on every grid -- with the default mask measured 24-27 % faster on periodic
+  // grids than the run-time-masked pair kernel below and 6 % faster than one node per thread
+  // on boxes (confined Hall 128^3)
+  if (sh.pairs && hall && conv && !foad && (hodp || !hod) &&
+      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 13 || a.need == 14 || a.need == 15) &&
+      a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) && pair_ok(a.Hpre) && pair_ok(a.X) &&
+      pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
+    switch (a.need) {
+      case 9: launch_hall_conv_pairs<9>(a, per, hodp, sh, s); break;
+      case 6: launch_hall_conv_pairs<6>(a, per, hodp, sh, s); break;
+      case 13: launch_hall_conv_pairs<13>(a, per, hodp, sh, s); break;
+      case 14: launch_hall_conv_pairs<14>(a, per, hodp, sh, s); break;
+      case 15: launch_hall_conv_pairs<15>(a, per, hodp, sh, s); break;
+      default: launch_hall_conv_pairs<10>(a, per, hodp, sh, s); break;
     }
     return;
   }

@@ -259,6 +259,18 @@ HALL_CONV_CASES = {
     # the same without the Hall term (convection and first-order dissipation only)
     "rotation_4c_conv_fo_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                                     dissipation="FIRST_ORDER", integrator="SSPRK33", dt=0.01, steps=2),
+    # Hall + convection with the masks of other flux forms (9, 15, 14), with the high-order
+    # dissipation precomputed on the periodic grid
+    "hallper_4c_hall_conv_czc_per": dict(order=4, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0, hi=HP_,
+                                         periodic=True, hall=True, uibj="CENTRAL", source="ZERO", ujbi="CENTRAL",
+                                         integrator="SSPRK33", dt=1e-3, steps=2),
+    "confined_4c_hall_conv_scs_box": dict(order=4, testcase="confined_domain", nodes=(16, 13, 14), lo=0.0, hi=1.0,
+                                          hall=True, uibj="SPLIT", source="CENTRAL", ujbi="SPLIT",
+                                          integrator="CarpenterKennedy2N54", dt=1e-5, steps=2),
+    "hallper_6c_hall_conv_hod_pcs_per": dict(order=6, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0,
+                                             hi=HP_, periodic=True, hall=True, dissipation="HIGH_ORDER",
+                                             uibj="PRODUCT", source="CENTRAL", ujbi="SPLIT", integrator="SSPRK33",
+                                             dt=1e-3, steps=2),
     # convection only with the two other flux forms of two sums per axis (masks 9 and 6)
     "rotation_4c_czc_box": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                                 uibj="CENTRAL", source="ZERO", ujbi="CENTRAL", integrator="SSPRK33", dt=0.01,
