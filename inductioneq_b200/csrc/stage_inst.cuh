@@ -248,12 +248,14 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   // grids than the run-time-masked pair kernel below and 6 % faster than one node per thread
   // on boxes (confined Hall 128^3)
   if (sh.pairs && hall && conv && !foad && (hodp || !hod) &&
-      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 13 || a.need == 14 || a.need == 15) &&
+      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 7 || a.need == 13 || a.need == 14 ||
+       a.need == 15) &&
       a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.E) && pair_ok(a.Hpre) && pair_ok(a.X) &&
       pair_ok(a.Y) && pair_ok(a.Z) && pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
     switch (a.need) {
       case 9: launch_hall_conv_pairs<9>(a, per, hodp, sh, s); break;
       case 6: launch_hall_conv_pairs<6>(a, per, hodp, sh, s); break;
+      case 7: launch_hall_conv_pairs<7>(a, per, hodp, sh, s); break;
       case 13: launch_hall_conv_pairs<13>(a, per, hodp, sh, s); break;
       case 14: launch_hall_conv_pairs<14>(a, per, hodp, sh, s); break;
       case 15: launch_hall_conv_pairs<15>(a, per, hodp, sh, s); break;
@@ -281,15 +283,17 @@ void launch_stage_col<IEQ_R, IEQ_OP>(const StageArgs<IEQ_R, SoA<IEQ_R>> &a, bool
   // per thread (rotation, orders 2/4/6, 64^3 .. 128^3).  Every other mask of the split forms
   // takes the same kernel with its own mask compiled in (two sums per axis: central u_i B_j
   // and u_j B_i with zero source, mask 9; product u_i B_j and u_j B_i with central source,
-  // mask 6; three or four sums, masks 13, 14, 15, at 3 blocks of <= 168 registers): measured
+  // mask 6; three or four sums, masks 7, 13, 14, 15, at 3 blocks of <= 168 registers): measured
   // 1.06-1.43x faster than one node per thread at 80^3 and 160^3 (rotation 3D, orders 2/4/6)
   if (sh.pairs && !hall && conv && !hod && !foad &&
-      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 13 || a.need == 14 || a.need == 15) &&
+      (a.need == 10 || a.need == 9 || a.need == 6 || a.need == 7 || a.need == 13 || a.need == 14 ||
+       a.need == 15) &&
       a.m.nx % 2 == 0 && pair_ok(a.bk) && pair_ok(a.u) && pair_ok(a.X) && pair_ok(a.Y) && pair_ok(a.Z) &&
       pair_ok(a.out) && pair_ok(a.out2) && pair_ok(a.out3)) {
     switch (a.need) {
       case 9: launch_conv_pairs<9>(a, per, sh, s); break;
       case 6: launch_conv_pairs<6>(a, per, sh, s); break;
+      case 7: launch_conv_pairs<7>(a, per, sh, s); break;
       case 13: launch_conv_pairs<13>(a, per, sh, s); break;
       case 14: launch_conv_pairs<14>(a, per, sh, s); break;
       case 15: launch_conv_pairs<15>(a, per, sh, s); break;

@@ -712,7 +712,7 @@ __device__ __forceinline__ void col_yz_pair(ColSums<R> (&s)[2], const StageArgs<
 #define IEQ_COL_X2_FO_MIN_BLOCKS 4
 #endif
 // resident blocks of the convection pair kernel with a compile-time flux-form mask: masks of
-// three or four sums per axis (13, 14, 15) get more registers (3 blocks of <= 168)
+// three or four sums per axis (7, 13, 14, 15) get more registers (3 blocks of <= 168)
 template <int NEED>
 __host__ __device__ constexpr int conv_min_blocks() {
   return (NEED >= 0 && ((NEED & 1) + ((NEED >> 1) & 1) + ((NEED >> 2) & 1) + ((NEED >> 3) & 1)) >= 3)
