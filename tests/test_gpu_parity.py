@@ -293,6 +293,12 @@ HALL_CONV_CASES = {
     "hallper_4c_hall_conv_csp_per": dict(order=4, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0, hi=HP_,
                                          periodic=True, hall=True, uibj="CENTRAL", source="SPLIT", ujbi="PRODUCT",
                                          integrator="SSPRK33", dt=1e-3, steps=2),
+    "rotation_4c_scs_box_f32": dict(order=4, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
+                                    uibj="SPLIT", source="CENTRAL", ujbi="SPLIT", integrator="SSPRK33", dt=0.01,
+                                    steps=2, real="float"),
+    "hallper_6c_hall_conv_czc_per_f32": dict(order=6, testcase="hall_periodic", nodes=(16, 12, 14), lo=0.0, hi=HP_,
+                                             periodic=True, hall=True, uibj="CENTRAL", source="ZERO",
+                                             ujbi="CENTRAL", integrator="SSPRK33", dt=1e-3, steps=2, real="float"),
     "rotation_2c_scs_box": dict(order=2, testcase="rotation_gaussian", nodes=(16, 13, 14), lo=-1.0, hi=1.0,
                                 uibj="SPLIT", source="CENTRAL", ujbi="SPLIT", integrator="SSPRK33", dt=0.01, steps=2),
     "rotation_6c_conv_fo_band": dict(order=6, testcase="rotation_gaussian", nodes=(20, 13, 14), lo=-1.0, hi=1.0,
